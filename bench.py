@@ -1,0 +1,342 @@
+"""DD3 projector / backprojector throughput on B200.
+
+One step = one branchless DD forward projection and one backprojection of
+the 512x512x256 volume over 984 views onto the 888x64 detector (the
+single-volume throughput workload): volume SATs + projection kernel,
+projection SATs + backprojection kernel.  value = voxel-views processed by
+both operators (2 * XN*YN*ZN*PN per step) per second, whole job, inputs
+resident in HBM.  e2e = the same metric through the reference-facing host
+entry points DD3Proj_gpu / DD3Back_gpu with pinned host buffers, copies
+included.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun), every rank projects and backprojects its own
+independent random-ellipsoid volume (weak scaling, no data-path collective);
+timing is the max over ranks.  --impl reference times the CPU restatement of
+the reference's DD path (the oracle) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DD3 proj+backproj throughput (Gvoxel-views/s)"
+UNIT = "Gvoxel-views/s"
+WORKLOAD = "dd3_proj_back_512x512x256_984v_888x64"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--sat", default="fp64", choices=["fp64", "f32pair"])
+    ap.add_argument("--cpu-views", type=int, default=4, help="views in the bounded CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def config_dict(args, extra=None):
+    d = {"workload": WORKLOAD, "volume": [512, 512, 256], "views": 984, "detector": [888, 64],
+         "voxel_mm": [1.0, 1.0, 0.15625], "cell_mm": [1.0239, 1.0960], "sod_sdd_mm": [541, 949],
+         "sat": args.sat, "l2": "inputs larger than L2 (volume 268 MB, SATs 1.08 GB)",
+         "phantom": "random ellipsoids, 20-40, seed 1+rank"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_sample(g, vol_h, prj_h, nviews):
+    """Oracle (CPU restatement) proj + back over a bounded view sample."""
+    import oracle
+    idx = np.linspace(0, g.PN - 1, nviews).round().astype(int)
+    gs = g.with_views(idx)
+    threads = oracle.num_threads()
+    t0 = time.perf_counter()
+    oracle.dd3_proj(gs, vol_h)
+    t1 = time.perf_counter()
+    oracle.dd3_back(gs, prj_h[idx])
+    t2 = time.perf_counter()
+    vv = g.XN * g.YN * g.ZN * nviews
+    return {"value": 2 * vv / (t2 - t0) / 1e9, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{nviews} evenly spaced views of the 984 (proj {t1 - t0:.1f} s + back {t2 - t1:.1f} s), "
+                      "FP64 oracle with OpenMP, scaled per voxel-view"}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    import oracle
+    from ctlab_b200 import geometry as G
+    g = G.config2()
+    hx, hy, hz = G.half_extents(g)
+    import ctlab_b200 as cb
+    ell = cb.random_ellipsoids(1, hx, hy, hz)
+    small = g.with_views(np.arange(2))
+    vol = oracle.ellipsoid_phantom(g, ell)
+    prj = oracle.dd3_proj(small, vol).astype(np.float32)
+    prj_all = np.zeros(g.prj_shape, np.float32)
+    prj_all[:2] = prj
+    nviews = max(1, args.cpu_views // 2)
+    for _ in range(args.warmup if args.warmup < 2 else 1):
+        pass
+    vals = []
+    for _ in range(max(1, args.steps)):
+        vals.append(cpu_sample(g, vol, prj_all, nviews)["value"])
+    v = float(np.median(vals))
+    threads = oracle.num_threads()
+    vv2 = 2 * g.voxel_views
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": vv2 / (v * 1e9) * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_dict(args), "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"each step: {nviews} evenly spaced views of 984, proj + back, FP64 oracle"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    import ctlab_b200 as cb
+    from ctlab_b200 import geometry as G
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        dist.init_process_group("nccl", init_method="env://", world_size=ws, rank=rank,
+                                timeout=__import__("datetime").timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    g = G.config2()
+    hx, hy, hz = G.half_extents(g)
+    ell = cb.random_ellipsoids(1 + rank, hx, hy, hz)
+    sat_mode = cb.CTLAB_SAT_FP64 if args.sat == "fp64" else cb.CTLAB_SAT_F32PAIR
+    plan = cb.Plan(g, device=local, sat_mode=sat_mode)
+    vol = torch.zeros(g.vol_shape, dtype=torch.float32, device="cuda")
+    cb.ellipsoid_phantom(vol, g, ell)
+    prj_in = torch.zeros(g.prj_shape, dtype=torch.float32, device="cuda")
+    plan.proj(vol, prj_in)
+    prj = torch.zeros_like(prj_in)
+    back = torch.zeros_like(vol)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        plan.proj(vol, prj)
+        plan.back(prj_in, back)
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    launches_per_step = 0
+    plan.proj(vol, prj)
+    launches_per_step += plan.last_launches()
+    plan.back(prj_in, back)
+    launches_per_step += plan.last_launches()
+    torch.cuda.synchronize()
+
+    # timed region: K steps, barrier + synchronize on both sides
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    if ws > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    vv = g.voxel_views
+    value = ws * 2 * vv / (ms_step * 1e-3) / 1e9
+
+    # per-kernel times (CUDA events inside the plan, on the launching stream)
+    plan.set_timing(True)
+    proj_sat, proj_k, back_sat, back_k = [], [], [], []
+    for _ in range(args.steps):
+        plan.proj(vol, prj)
+        a, b = plan.last_times()
+        proj_sat.append(a)
+        proj_k.append(b)
+        plan.back(prj_in, back)
+        a, b = plan.last_times()
+        back_sat.append(a)
+        back_k.append(b)
+    plan.set_timing(False)
+    t_proj, t_back = float(np.mean(proj_k)), float(np.mean(back_k))
+    peak, peak_kind = peaks()
+    alg = 8.0 * vv + 4.0 * g.PN * g.DNU * g.DNV  # bytes per launch (proj or back)
+    dom = "dd3_proj_kernel" if t_proj >= t_back else "dd3_back_kernel"
+    t_dom = max(t_proj, t_back)
+    achieved = alg / (t_dom * 1e-3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "dram_bytes.json")
+    if os.path.exists(tp):
+        traffic = json.load(open(tp)).get(dom)
+
+    # e2e through the host entry points with pinned buffers
+    e2e = None
+    if not args.no_e2e:
+        hvol = torch.empty(g.vol_shape, dtype=torch.float32, pin_memory=True)
+        hvol.copy_(vol.cpu())
+        hprj = torch.empty(g.prj_shape, dtype=torch.float32, pin_memory=True)
+        hback = torch.empty(g.vol_shape, dtype=torch.float32, pin_memory=True)
+        hv, hp, hb = hvol.numpy(), hprj.numpy(), hback.numpy()
+        gargs = g.args()
+
+        def e2e_step():
+            cb.DD3Proj_gpu(**gargs, hvol=hv, hprj=hp, mask=None, gpunum=local, prjMode=0)
+            cb.DD3Back_gpu(**gargs, hvol=hb, hprj=hp, mask=None, gpunum=local, squared=0, prjMode=0)
+
+        for _ in range(max(2, args.warmup)):
+            e2e_step()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        t1 = time.perf_counter()
+        barrier()
+        es = (t1 - t0) / args.steps
+        if ws > 1:
+            t = torch.tensor([es], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            es = float(t.item())
+        nvb, npb = 4 * vv // g.PN, 4 * g.PN * g.DNU * g.DNV
+        e2e = {"value": ws * 2 * vv / es / 1e9, "unit": UNIT, "h2d_bytes_per_step": nvb + npb,
+               "d2h_bytes_per_step": npb + nvb, "ms_per_step": es * 1e3,
+               "path": "DD3Proj_gpu + DD3Back_gpu (host pointers, pinned)"}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_sample(g, vol.cpu().numpy(), prj_in.cpu().numpy(), args.cpu_views)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (f64 SAT)" if args.sat == "fp64" else "f32 (f32-pair SAT)",
+            "data": "synthetic (seeded random-ellipsoid phantoms)",
+            "config": config_dict(args, {"parallelism": f"independent volume per GPU x{ws}"}),
+            "clocks": clk.summary(),
+            "e2e": e2e,
+            "gpu_launches": launches_per_step * args.steps,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                         "traffic": traffic, "algorithmic_bytes_per_launch": alg,
+                         "launch_ms": t_dom},
+            "kernels_ms": {"proj_sat": float(np.mean(proj_sat)), "proj": t_proj,
+                           "back_sat": float(np.mean(back_sat)), "back": t_back},
+            "proj_gvvps": vv / (t_proj + float(np.mean(proj_sat))) / 1e6,
+            "back_gvvps": vv / (t_back + float(np.mean(back_sat))) / 1e6,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,212 @@
+// Internal declarations shared by the libctlab_b200 translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/ctlab_b200.h"
+
+namespace ctlab {
+
+// ----------------------------------------------------------------------
+// status handling: every C entry point funnels through these
+// ----------------------------------------------------------------------
+int set_status(int code, const std::string &msg);
+inline int ok() { return set_status(CTLAB_OK, ""); }
+int cuda_status(cudaError_t e, const char *what);
+
+#define CTLAB_CUDA_TRY(expr)                                                   \
+    do {                                                                       \
+        cudaError_t _e = (expr);                                               \
+        if (_e != cudaSuccess) return ::ctlab::cuda_status(_e, #expr);         \
+    } while (0)
+
+// Restores the caller's current device on scope exit.
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = false;
+    explicit DeviceGuard(int dev);
+    ~DeviceGuard();
+};
+
+// ----------------------------------------------------------------------
+// geometry
+// ----------------------------------------------------------------------
+
+// Per-view constants computed on the host in FP64.  (a, b) are the
+// driving axis and the other in-plane axis of the view: a = y, b = x for
+// y-driven views (slices y = const, SAT_y), a = x, b = y for x-driven.
+struct DevView {
+    double c, s;       // cos / sin of the regularised angle
+    double Sx, Sy, Sz; // source, world
+    double Sa, Sb;     // source along a and b
+    double a0;         // a coordinate of slice 0's centre
+    double b_lo;       // b coordinate of in-plane boundary 0
+    double zP;         // z shift of the view
+    double B0x, B0y;   // detector u-boundary 0, world (flat detectors)
+    double Ex, Ey;     // detector u pitch vector, world (flat detectors)
+    int xdrv;          // 1: x-driven
+    int na, nb;        // slices along a, voxels along b
+    int pad;
+};
+
+// Host-side description of a validated scan.
+struct HostGeometry {
+    double x0, y0, z0;
+    int DNU, DNV, PN, XN, YN, ZN;
+    double cx, cy, cz, dx, dz;
+    double x_lo, y_lo, z_lo; // voxel boundary 0 along x, y, z
+    std::vector<double> bx, by, bz; // local detector boundaries (DNU+1, DNU+1, DNV+1)
+    std::vector<double> ux, uy, vz; // local detector centres (DNU, DNU, DNV)
+    std::vector<DevView> views;
+    bool flat_uniform = false; // flat detector with uniform u and v pitch
+    double dzb = 0;            // v pitch (flat_uniform)
+};
+
+// Validates and converts the ctlab_geometry; returns CTLAB_OK or an error
+// code with the message recorded.
+int build_geometry(const ctlab_geometry &g, HostGeometry &out);
+
+// Detector table on the device, doubles:
+//   [0, DNU+1)         bx      local u-boundaries x
+//   [DNU+1, 2(DNU+1))  by      local u-boundaries y
+//   next DNU           ux      local centres x
+//   next DNU           uy      local centres y
+//   next DNV+1         bz      local z boundaries
+//   next DNV           vz      local z centres
+struct DetTable {
+    int off_bx, off_by, off_ux, off_uy, off_bz, off_vz, total;
+};
+__host__ __device__ inline DetTable det_table_layout(int DNU, int DNV)
+{
+    DetTable t;
+    t.off_bx = 0;
+    t.off_by = t.off_bx + DNU + 1;
+    t.off_ux = t.off_by + DNU + 1;
+    t.off_uy = t.off_ux + DNU;
+    t.off_bz = t.off_uy + DNU;
+    t.off_vz = t.off_bz + DNV + 1;
+    t.total = t.off_vz + DNV;
+    return t;
+}
+std::vector<double> det_table_host(const HostGeometry &g);
+
+// ----------------------------------------------------------------------
+// kernels (launchers return cudaError_t from the launch)
+// ----------------------------------------------------------------------
+
+// Lookback state for the chunked SAT scans: per (plane, chunk) a status flag,
+// an aggregate vector and an inclusive-prefix vector.
+struct ScanState {
+    int *ticket;    // one counter per launch, zeroed before the launch
+    int *flags;     // [planes * chunks]
+    double *agg;    // [planes * chunks * nk]
+    double *pref;   // [planes * chunks * nk]
+    int *err;       // device error word (timeouts)
+};
+
+size_t scan_state_doubles(int planes, int chunks, int nk);
+// Number of chunks the scan of ns rows of nk elements uses for a requested chunk.
+int scan_chunks(int ns, int nk, int chunk, int f32pair);
+
+// Volume SAT of one orientation (0: y-slices over (x,z) planes -> SAT_y,
+// 1: x-slices over (y,z) planes -> SAT_x), FP64 or float-pair output.
+cudaError_t launch_volume_sat(const float *vol, const unsigned char *mask, int XN, int YN, int ZN,
+                              int orientation, void *out, int zp, int f32pair, ScanState st,
+                              int chunk, cudaStream_t s);
+
+// Projection SAT: Q[p][u'][v'] of W = prj * L (L = slab path weight of the
+// view's driving axis) for n views of the list.
+struct ProjSatArgs {
+    const float *prj;     // [n][DNU][DNV]
+    const DevView *views; // plan views
+    const int *view_list; // [n] (device)
+    int n;
+    const double *det;    // detector table
+    int DNU, DNV;
+    double dx;
+    void *out;            // [n][DNU+1][vp]
+    int vp;
+    int f32pair;
+};
+cudaError_t launch_proj_sat(const ProjSatArgs &a, ScanState st, int chunk, cudaStream_t s);
+// Diagnostics: a scan whose first chunk never publishes (see ctlab_debug_scan_stall).
+cudaError_t launch_scan_stall(const float *vol, int rows, int nk, void *out, ScanState st, int chunk,
+                              unsigned spin_limit, cudaStream_t s);
+
+enum ProjEpilogue { PROJ_PLAIN = 0, PROJ_SART_RESIDUAL = 1 };
+
+struct ProjArgs {
+    const void *sat_y; // [YN][XN+1][zp]
+    const void *sat_x; // [XN][YN+1][zp]
+    int zp;
+    int XN, YN, ZN;
+    double dx, dz, z_lo;
+    const DevView *views;
+    const int *view_list; // [n] (device)
+    int n;
+    const double *det;
+    int DNU, DNV;
+    float *out;           // [n][DNU][DNV]
+    int f32pair;
+    int epilogue;
+    const float *meas;    // [n][DNU][DNV]  (SART residual)
+    const float *row_sum; // [n][DNU][DNV]
+    double *resid2;       // accumulates sum (meas - Ax)^2 and sum meas^2
+};
+cudaError_t launch_proj(const ProjArgs &a, cudaStream_t s, int *launches);
+bool proj_supported(int ZN, int DNV);
+
+enum BackEpilogue { BACK_PLAIN = 0, BACK_SART_UPDATE = 1 };
+
+struct BackArgs {
+    const void *q;        // [n][DNU+1][vp] projection SATs
+    int vp;
+    const DevView *views;
+    const int *view_list;
+    int n;
+    const double *det;
+    int DNU, DNV;
+    double dzb;           // detector v pitch
+    int XN, YN, ZN;
+    double dx, dz, x_c0, y_c0, z_lo;  // centres of voxel 0 along x, y; z boundary 0
+    const unsigned char *mask;
+    float *out;           // volume
+    int f32pair;
+    int epilogue;
+    const float *col_sum; // SART update
+    float lambda;
+    int clamp;
+    float min_v, max_v;
+};
+cudaError_t launch_back(const BackArgs &a, cudaStream_t s, int *launches);
+bool back_supported(int DNV);
+
+// elementwise
+cudaError_t launch_sart_proj_weight(float *prj, const float *real, const float *row_sum, long long n,
+                                    cudaStream_t s);
+cudaError_t launch_sart_back_weight(float *vol, float *recon, const float *col_sum, long long n,
+                                    cudaStream_t s);
+cudaError_t launch_fista_step(const float *las, float *cur, float t1, float t2, long long n,
+                              float min_v, float max_v, cudaStream_t s);
+cudaError_t launch_tv_gradient(const float *f, float *g, int XN, int YN, int ZN, float eps,
+                               cudaStream_t s);
+cudaError_t launch_fill(float *p, float v, long long n, cudaStream_t s);
+cudaError_t launch_mask_fill(float *p, const unsigned char *mask, long long ncols, int ZN, cudaStream_t s);
+// x = (z - lam * g) * mask ; and the SART-preconditioned step y += q/colSum
+cudaError_t launch_tv_step(float *x, const float *z, const float *g, const unsigned char *mask, float lam,
+                           long long n, int ZN, cudaStream_t s);
+cudaError_t launch_add_scaled_div(float *y, const float *q, const float *col_sum, long long n, cudaStream_t s);
+// gathers b[list[i]] views into out (subset-major copy)
+cudaError_t launch_gather_views(const float *src, const int *list, int n, long long view_elems, float *dst,
+                                cudaStream_t s);
+// sum of squares of (a - b) and of a (double accumulators)
+cudaError_t launch_resid2(const float *meas, const float *est, long long n, double *acc, cudaStream_t s);
+
+cudaError_t launch_phantom(float *vol, int XN, int YN, int ZN, float dx, float dz, float cx, float cy,
+                           float cz, const float *ell_dev, int n_ell, int clamp_nonneg, cudaStream_t s);
+
+} // namespace ctlab

@@ -1,0 +1,458 @@
+// Plans and the device-pointer C ABI: geometry upload, SAT workspaces,
+// stream-ordered projection / backprojection.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <new>
+
+#include "plan.h"
+
+using namespace ctlab;
+
+namespace ctlab {
+
+namespace {
+
+constexpr int kVolChunk = 32;  // rows per CTA of the volume SAT scans
+constexpr int kPrjChunk = 32;  // rows per CTA of the projection SAT scans
+
+int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+template <class T>
+cudaError_t dmalloc(T **p, size_t n, long long &bytes)
+{
+    *p = nullptr;
+    if (n == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+    if (e == cudaSuccess) bytes += (long long)(n * sizeof(T));
+    return e;
+}
+
+} // namespace
+
+void plan_free(ctlab_plan *p)
+{
+    if (!p) return;
+    DeviceGuard g(p->device);
+    void *bufs[] = {p->d_views, p->d_det, p->d_all_views, p->d_list, p->d_sat_y, p->d_sat_x,
+                    p->d_q, p->d_ticket, p->d_flags, p->d_agg, p->d_pref, p->d_err};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    for (auto &e : p->ev)
+        if (e) cudaEventDestroy(e);
+    delete p;
+}
+
+int plan_volume_sat(ctlab_plan *p, const float *d_vol, const unsigned char *d_mask, cudaStream_t s)
+{
+    const HostGeometry &g = p->g;
+    ScanState st{p->d_ticket, p->d_flags, p->d_agg, p->d_pref, p->d_err};
+    if (p->need_y) {
+        cudaError_t e = launch_volume_sat(d_vol, d_mask, g.XN, g.YN, g.ZN, 0, p->d_sat_y, p->zp, p->sat_mode,
+                                          st, kVolChunk, s);
+        if (e != cudaSuccess) return cuda_status(e, "volume SAT (y slices)");
+        ++p->last_launches;
+    }
+    if (p->need_x) {
+        cudaError_t e = launch_volume_sat(d_vol, d_mask, g.XN, g.YN, g.ZN, 1, p->d_sat_x, p->zp, p->sat_mode,
+                                          st, kVolChunk, s);
+        if (e != cudaSuccess) return cuda_status(e, "volume SAT (x slices)");
+        ++p->last_launches;
+    }
+    return CTLAB_OK;
+}
+
+int plan_proj_list(ctlab_plan *p, const int *d_list, int n, float *d_prj, cudaStream_t s, int epilogue,
+                   const float *meas, const float *row_sum, double *resid2)
+{
+    const HostGeometry &g = p->g;
+    ProjArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.sat_y = p->d_sat_y;
+    a.sat_x = p->d_sat_x;
+    a.zp = p->zp;
+    a.XN = g.XN; a.YN = g.YN; a.ZN = g.ZN;
+    a.dx = g.dx; a.dz = g.dz; a.z_lo = g.z_lo;
+    a.views = p->d_views;
+    a.view_list = d_list;
+    a.n = n;
+    a.det = p->d_det;
+    a.DNU = g.DNU; a.DNV = g.DNV;
+    a.out = d_prj;
+    a.f32pair = p->sat_mode;
+    a.epilogue = epilogue;
+    a.meas = meas;
+    a.row_sum = row_sum;
+    a.resid2 = resid2;
+    cudaError_t e = launch_proj(a, s, &p->last_launches);
+    if (e != cudaSuccess) return cuda_status(e, "DD3 projection kernel");
+    return CTLAB_OK;
+}
+
+int plan_proj_sat(ctlab_plan *p, const int *d_list, int n, const float *d_prj, cudaStream_t s)
+{
+    const HostGeometry &g = p->g;
+    if (n > p->q_capacity) return set_status(CTLAB_ERR_INTERNAL, "projection SAT capacity exceeded");
+    ProjSatArgs a;
+    a.prj = d_prj;
+    a.views = p->d_views;
+    a.view_list = d_list;
+    a.n = n;
+    a.det = p->d_det;
+    a.DNU = g.DNU; a.DNV = g.DNV;
+    a.dx = g.dx;
+    a.out = p->d_q;
+    a.vp = p->vp;
+    a.f32pair = p->sat_mode;
+    ScanState st{p->d_ticket, p->d_flags, p->d_agg, p->d_pref, p->d_err};
+    cudaError_t e = launch_proj_sat(a, st, kPrjChunk, s);
+    if (e != cudaSuccess) return cuda_status(e, "projection SAT");
+    ++p->last_launches;
+    return CTLAB_OK;
+}
+
+int plan_back_list(ctlab_plan *p, const int *d_list, int n, const unsigned char *d_mask, float *d_vol,
+                   cudaStream_t s, int epilogue, const float *col_sum, float lambda, int clamp, float min_v,
+                   float max_v)
+{
+    const HostGeometry &g = p->g;
+    BackArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.q = p->d_q;
+    a.vp = p->vp;
+    a.views = p->d_views;
+    a.view_list = d_list;
+    a.n = n;
+    a.det = p->d_det;
+    a.DNU = g.DNU; a.DNV = g.DNV;
+    a.dzb = g.dzb;
+    a.XN = g.XN; a.YN = g.YN; a.ZN = g.ZN;
+    a.dx = g.dx; a.dz = g.dz;
+    a.x_c0 = g.cx - 0.5 * (g.XN - 1) * g.dx;
+    a.y_c0 = g.cy - 0.5 * (g.YN - 1) * g.dx;
+    a.z_lo = g.z_lo;
+    a.mask = d_mask;
+    a.out = d_vol;
+    a.f32pair = p->sat_mode;
+    a.epilogue = epilogue;
+    a.col_sum = col_sum;
+    a.lambda = lambda;
+    a.clamp = clamp;
+    a.min_v = min_v;
+    a.max_v = max_v;
+    if (n == 0 && epilogue == BACK_PLAIN) {
+        CTLAB_CUDA_TRY(cudaMemsetAsync(d_vol, 0, sizeof(float) * (size_t)g.XN * g.YN * g.ZN, s));
+        return CTLAB_OK;
+    }
+    cudaError_t e = launch_back(a, s, &p->last_launches);
+    if (e != cudaSuccess) return cuda_status(e, "DD3 backprojection kernel");
+    return CTLAB_OK;
+}
+
+int plan_upload_list(ctlab_plan *p, const int *h_views, int n, cudaStream_t s)
+{
+    if (n < 0 || n > p->g.PN) return set_status(CTLAB_ERR_INVALID_ARG, "view count out of range");
+    for (int i = 0; i < n; ++i)
+        if (h_views[i] < 0 || h_views[i] >= p->g.PN)
+            return set_status(CTLAB_ERR_INVALID_ARG, "view index out of range");
+    if (n == 0) return CTLAB_OK;
+    // The list buffer is re-used by the next call on the same stream only
+    // after this call's kernels, because the copy is stream-ordered; the
+    // host array is staged so the caller may free it at once.
+    p->h_list.assign(h_views, h_views + n);
+    CTLAB_CUDA_TRY(cudaMemcpyAsync(p->d_list, p->h_list.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, s));
+    CTLAB_CUDA_TRY(cudaStreamSynchronize(s));
+    return CTLAB_OK;
+}
+
+int plan_check_device_error(ctlab_plan *p, cudaStream_t s)
+{
+    int err = 0;
+    CTLAB_CUDA_TRY(cudaMemcpyAsync(&err, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CTLAB_CUDA_TRY(cudaStreamSynchronize(s));
+    if (err != 0) {
+        cudaMemsetAsync(p->d_err, 0, sizeof(int), s);
+        cudaStreamSynchronize(s);
+        return set_status(CTLAB_ERR_TIMEOUT, "a bounded wait in a SAT scan timed out; results are invalid");
+    }
+    return CTLAB_OK;
+}
+
+void timing_mark(ctlab_plan *p, int which, cudaStream_t s)
+{
+    if (p->timing) cudaEventRecord(p->ev[which], s);
+}
+
+} // namespace ctlab
+
+extern "C" {
+
+int ctlab_plan_create(const ctlab_geometry *geom, int device, int sat_mode, ctlab_plan **out)
+{
+    if (!geom || !out) return set_status(CTLAB_ERR_INVALID_ARG, "null geometry or output pointer");
+    *out = nullptr;
+    if (sat_mode != CTLAB_SAT_FP64 && sat_mode != CTLAB_SAT_F32PAIR)
+        return set_status(CTLAB_ERR_INVALID_ARG, "sat_mode must be CTLAB_SAT_FP64 or CTLAB_SAT_F32PAIR");
+    ctlab_plan *p = new (std::nothrow) ctlab_plan();
+    if (!p) return set_status(CTLAB_ERR_OOM, "host allocation failed");
+    int rc = build_geometry(*geom, p->g);
+    if (rc != CTLAB_OK) {
+        delete p;
+        return rc;
+    }
+    const HostGeometry &g = p->g;
+    if (!proj_supported(g.ZN, g.DNV)) {
+        delete p;
+        return set_status(CTLAB_ERR_UNSUPPORTED, "ZN or DNV beyond the projector's shared-memory tiles");
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        delete p;
+        return set_status(CTLAB_ERR_INVALID_ARG, "no such CUDA device");
+    }
+    p->device = device;
+    p->sat_mode = sat_mode;
+    DeviceGuard dg(device);
+    if (!dg.ok) {
+        delete p;
+        return set_status(CTLAB_ERR_CUDA, "cudaSetDevice failed");
+    }
+    for (const auto &v : g.views) (v.xdrv ? p->need_x : p->need_y) = true;
+    p->zp = round_up(g.ZN + 1, 2);
+    p->vp = round_up(g.DNV + 1, 2);
+    p->q_capacity = g.PN;
+
+    long long &bytes = p->bytes;
+    cudaError_t e = cudaSuccess;
+    auto chk = [&](cudaError_t r) {
+        if (e == cudaSuccess) e = r;
+    };
+    chk(dmalloc(&p->d_views, g.views.size(), bytes));
+    std::vector<double> det = det_table_host(g);
+    chk(dmalloc(&p->d_det, det.size(), bytes));
+    chk(dmalloc(&p->d_all_views, (size_t)g.PN, bytes));
+    chk(dmalloc(&p->d_list, (size_t)g.PN, bytes));
+    const size_t esz = 8; // double or float pair
+    if (p->need_y) chk(dmalloc((char **)&p->d_sat_y, esz * (size_t)g.YN * (g.XN + 1) * p->zp, bytes));
+    if (p->need_x) chk(dmalloc((char **)&p->d_sat_x, esz * (size_t)g.XN * (g.YN + 1) * p->zp, bytes));
+    if (back_supported(g.DNV) && g.flat_uniform)
+        chk(dmalloc((char **)&p->d_q, esz * (size_t)g.PN * (g.DNU + 1) * p->vp, bytes));
+    else
+        p->q_capacity = 0;
+    // lookback state sized for the largest scan
+    size_t tiles = 0, state = 0;
+    auto need = [&](int planes, int ns, int nk, int chunk) {
+        const int c = scan_chunks(ns, nk, chunk, sat_mode);
+        tiles = std::max(tiles, (size_t)planes * c);
+        state = std::max(state, scan_state_doubles(planes, c, nk));
+    };
+    if (p->need_y) need(g.YN, g.XN, g.ZN, kVolChunk);
+    if (p->need_x) need(g.XN, g.YN, g.ZN, kVolChunk);
+    if (p->q_capacity) need(g.PN, g.DNU, g.DNV, kPrjChunk);
+    chk(dmalloc(&p->d_ticket, 1, bytes));
+    chk(dmalloc(&p->d_flags, tiles, bytes));
+    chk(dmalloc(&p->d_agg, state, bytes));
+    chk(dmalloc(&p->d_pref, state, bytes));
+    chk(dmalloc(&p->d_err, 1, bytes));
+    if (e != cudaSuccess) {
+        plan_free(p);
+        return cuda_status(e, "plan workspace allocation");
+    }
+    std::vector<int> all(g.PN);
+    for (int i = 0; i < g.PN; ++i) all[i] = i;
+    chk(cudaMemcpy(p->d_views, g.views.data(), sizeof(DevView) * g.views.size(), cudaMemcpyHostToDevice));
+    chk(cudaMemcpy(p->d_det, det.data(), sizeof(double) * det.size(), cudaMemcpyHostToDevice));
+    chk(cudaMemcpy(p->d_all_views, all.data(), sizeof(int) * all.size(), cudaMemcpyHostToDevice));
+    chk(cudaMemset(p->d_err, 0, sizeof(int)));
+    for (auto &ev : p->ev) chk(cudaEventCreate(&ev));
+    if (e != cudaSuccess) {
+        plan_free(p);
+        return cuda_status(e, "plan upload");
+    }
+    *out = p;
+    return ok();
+}
+
+int ctlab_plan_destroy(ctlab_plan *plan)
+{
+    plan_free(plan);
+    return ok();
+}
+
+long long ctlab_plan_workspace_bytes(const ctlab_plan *plan) { return plan ? plan->bytes : 0; }
+
+int ctlab_plan_set_timing(ctlab_plan *plan, int enable)
+{
+    if (!plan) return set_status(CTLAB_ERR_INVALID_ARG, "null plan");
+    plan->timing = enable != 0;
+    return ok();
+}
+
+int ctlab_plan_last_times(ctlab_plan *plan, float *sat_ms, float *gather_ms)
+{
+    if (!plan || !sat_ms || !gather_ms) return set_status(CTLAB_ERR_INVALID_ARG, "null argument");
+    if (!plan->timing) return set_status(CTLAB_ERR_INVALID_ARG, "timing is not enabled on this plan");
+    DeviceGuard dg(plan->device);
+    CTLAB_CUDA_TRY(cudaEventSynchronize(plan->ev[2]));
+    CTLAB_CUDA_TRY(cudaEventElapsedTime(sat_ms, plan->ev[0], plan->ev[1]));
+    CTLAB_CUDA_TRY(cudaEventElapsedTime(gather_ms, plan->ev[1], plan->ev[2]));
+    return ok();
+}
+
+int ctlab_plan_last_launches(const ctlab_plan *plan) { return plan ? plan->last_launches : -1; }
+
+int ctlab_plan_sat_layout(const ctlab_plan *plan, int orientation, int *planes, int *rows, int *zp)
+{
+    if (!plan || !planes || !rows || !zp) return set_status(CTLAB_ERR_INVALID_ARG, "null argument");
+    const HostGeometry &g = plan->g;
+    if (orientation == 0 && plan->need_y) {
+        *planes = g.YN; *rows = g.XN + 1;
+    } else if (orientation == 1 && plan->need_x) {
+        *planes = g.XN; *rows = g.YN + 1;
+    } else {
+        return set_status(CTLAB_ERR_INVALID_ARG, "orientation not used by this plan's views");
+    }
+    *zp = plan->zp;
+    return ok();
+}
+
+int ctlab_copy_volume_sat(ctlab_plan *plan, int orientation, void *d_out, void *stream)
+{
+    int planes, rows, zp;
+    int rc = ctlab_plan_sat_layout(plan, orientation, &planes, &rows, &zp);
+    if (rc != CTLAB_OK) return rc;
+    if (!d_out) return set_status(CTLAB_ERR_INVALID_ARG, "null output");
+    DeviceGuard dg(plan->device);
+    const void *src = orientation == 0 ? plan->d_sat_y : plan->d_sat_x;
+    CTLAB_CUDA_TRY(cudaMemcpyAsync(d_out, src, 8 * (size_t)planes * rows * zp, cudaMemcpyDeviceToDevice,
+                                   (cudaStream_t)stream));
+    return ok();
+}
+
+int ctlab_volume_sat(ctlab_plan *plan, const float *d_vol, const unsigned char *d_mask, void *stream)
+{
+    if (!plan || !d_vol) return set_status(CTLAB_ERR_INVALID_ARG, "null plan or volume");
+    DeviceGuard dg(plan->device);
+    plan->last_launches = 0;
+    int rc = plan_volume_sat(plan, d_vol, d_mask, (cudaStream_t)stream);
+    return rc == CTLAB_OK ? ok() : rc;
+}
+
+int ctlab_proj(ctlab_plan *plan, const float *d_vol, const unsigned char *d_mask, float *d_prj, void *stream)
+{
+    if (!plan || !d_vol || !d_prj) return set_status(CTLAB_ERR_INVALID_ARG, "null plan, volume or projection");
+    std::lock_guard<std::mutex> lk(plan->mu);
+    DeviceGuard dg(plan->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    plan->last_launches = 0;
+    timing_mark(plan, 0, s);
+    int rc = plan_volume_sat(plan, d_vol, d_mask, s);
+    if (rc != CTLAB_OK) return rc;
+    timing_mark(plan, 1, s);
+    rc = plan_proj_list(plan, plan->d_all_views, plan->g.PN, d_prj, s, PROJ_PLAIN, nullptr, nullptr, nullptr);
+    if (rc != CTLAB_OK) return rc;
+    timing_mark(plan, 2, s);
+    return ok();
+}
+
+int ctlab_proj_views(ctlab_plan *plan, const int *h_views, int n, const float *d_vol,
+                     const unsigned char *d_mask, float *d_prj, void *stream)
+{
+    if (!plan || !h_views || !d_vol || !d_prj) return set_status(CTLAB_ERR_INVALID_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(plan->mu);
+    DeviceGuard dg(plan->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    plan->last_launches = 0;
+    int rc = plan_upload_list(plan, h_views, n, s);
+    if (rc != CTLAB_OK) return rc;
+    if (n == 0) return ok();
+    timing_mark(plan, 0, s);
+    rc = plan_volume_sat(plan, d_vol, d_mask, s);
+    if (rc != CTLAB_OK) return rc;
+    timing_mark(plan, 1, s);
+    rc = plan_proj_list(plan, plan->d_list, n, d_prj, s, PROJ_PLAIN, nullptr, nullptr, nullptr);
+    if (rc != CTLAB_OK) return rc;
+    timing_mark(plan, 2, s);
+    return ok();
+}
+
+static int back_common(ctlab_plan *plan, const int *d_list, int n, const float *d_prj,
+                       const unsigned char *d_mask, float *d_vol, cudaStream_t s)
+{
+    if (!plan->g.flat_uniform)
+        return set_status(CTLAB_ERR_UNSUPPORTED,
+                          "backprojection needs a flat detector with uniform u and v pitch");
+    if (plan->q_capacity == 0)
+        return set_status(CTLAB_ERR_UNSUPPORTED, "DNV beyond the backprojector's shared-memory tiles");
+    timing_mark(plan, 0, s);
+    int rc = CTLAB_OK;
+    if (n > 0) rc = plan_proj_sat(plan, d_list, n, d_prj, s);
+    if (rc != CTLAB_OK) return rc;
+    timing_mark(plan, 1, s);
+    rc = plan_back_list(plan, d_list, n, d_mask, d_vol, s, BACK_PLAIN, nullptr, 1.f, 0, 0.f, 0.f);
+    if (rc != CTLAB_OK) return rc;
+    timing_mark(plan, 2, s);
+    return ok();
+}
+
+int ctlab_back(ctlab_plan *plan, const float *d_prj, const unsigned char *d_mask, float *d_vol, void *stream)
+{
+    if (!plan || !d_prj || !d_vol) return set_status(CTLAB_ERR_INVALID_ARG, "null plan, projection or volume");
+    std::lock_guard<std::mutex> lk(plan->mu);
+    DeviceGuard dg(plan->device);
+    plan->last_launches = 0;
+    return back_common(plan, plan->d_all_views, plan->g.PN, d_prj, d_mask, d_vol, (cudaStream_t)stream);
+}
+
+int ctlab_back_views(ctlab_plan *plan, const int *h_views, int n, const float *d_prj,
+                     const unsigned char *d_mask, float *d_vol, void *stream)
+{
+    if (!plan || !h_views || !d_prj || !d_vol) return set_status(CTLAB_ERR_INVALID_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(plan->mu);
+    DeviceGuard dg(plan->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    plan->last_launches = 0;
+    int rc = plan_upload_list(plan, h_views, n, s);
+    if (rc != CTLAB_OK) return rc;
+    return back_common(plan, plan->d_list, n, d_prj, d_mask, d_vol, s);
+}
+
+} // extern "C"
+
+extern "C" int ctlab_debug_scan_stall(int device, unsigned spin_limit)
+{
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+        return set_status(CTLAB_ERR_INVALID_ARG, "no such CUDA device");
+    if (spin_limit < 1 || spin_limit > (1u << 24))
+        return set_status(CTLAB_ERR_INVALID_ARG, "spin_limit must be in [1, 2^24]");
+    DeviceGuard dg(device);
+    const int rows = 2, nk = 8;
+    float *vol = nullptr;
+    double *out = nullptr, *agg = nullptr, *pref = nullptr;
+    int *ticket = nullptr, *flags = nullptr, *err = nullptr;
+    cudaError_t e = cudaMalloc(&vol, sizeof(float) * rows * nk);
+    if (e == cudaSuccess) e = cudaMalloc(&out, sizeof(double) * (rows + 1) * (nk + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&agg, sizeof(double) * rows * nk);
+    if (e == cudaSuccess) e = cudaMalloc(&pref, sizeof(double) * rows * nk);
+    if (e == cudaSuccess) e = cudaMalloc(&ticket, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&flags, sizeof(int) * rows);
+    if (e == cudaSuccess) e = cudaMalloc(&err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(vol, 0, sizeof(float) * rows * nk);
+    if (e == cudaSuccess) e = cudaMemset(err, 0, sizeof(int));
+    int h_err = 0;
+    if (e == cudaSuccess) {
+        ScanState st{ticket, flags, agg, pref, err};
+        e = launch_scan_stall(vol, rows, nk, out, st, 1, spin_limit, 0);
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost);
+    void *bufs[] = {vol, out, agg, pref, ticket, flags, err};
+    for (void *b : bufs)
+        if (b) cudaFree(b);
+    if (e != cudaSuccess) return cuda_status(e, "scan stall diagnostic");
+    if (h_err == CTLAB_ERR_TIMEOUT)
+        return set_status(CTLAB_ERR_TIMEOUT, "bounded wait ran out as intended; the launch terminated");
+    return set_status(CTLAB_ERR_INTERNAL, "the stalled scan did not report a timeout");
+}

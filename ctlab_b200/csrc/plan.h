@@ -1,0 +1,47 @@
+// The plan object behind the C ABI's ctlab_plan handle.
+#pragma once
+
+#include <mutex>
+#include <vector>
+
+#include "internal.h"
+
+struct ctlab_plan {
+    int device = 0;
+    int sat_mode = CTLAB_SAT_FP64;
+    ctlab::HostGeometry g;
+    ctlab::DevView *d_views = nullptr;
+    double *d_det = nullptr;
+    int *d_all_views = nullptr; // 0..PN-1
+    int *d_list = nullptr;      // staged view list [PN]
+    std::vector<int> h_list;
+    bool need_y = false, need_x = false;
+    void *d_sat_y = nullptr, *d_sat_x = nullptr;
+    int zp = 0;
+    void *d_q = nullptr; // projection SATs [q_capacity][DNU+1][vp]
+    int vp = 0;
+    int q_capacity = 0;
+    int *d_ticket = nullptr, *d_flags = nullptr, *d_err = nullptr;
+    double *d_agg = nullptr, *d_pref = nullptr;
+    bool timing = false;
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    int last_launches = 0;
+    long long bytes = 0;
+    std::mutex mu;
+};
+
+namespace ctlab {
+
+void plan_free(ctlab_plan *p);
+int plan_volume_sat(ctlab_plan *p, const float *d_vol, const unsigned char *d_mask, cudaStream_t s);
+int plan_proj_list(ctlab_plan *p, const int *d_list, int n, float *d_prj, cudaStream_t s, int epilogue,
+                   const float *meas, const float *row_sum, double *resid2);
+int plan_proj_sat(ctlab_plan *p, const int *d_list, int n, const float *d_prj, cudaStream_t s);
+int plan_back_list(ctlab_plan *p, const int *d_list, int n, const unsigned char *d_mask, float *d_vol,
+                   cudaStream_t s, int epilogue, const float *col_sum, float lambda, int clamp, float min_v,
+                   float max_v);
+int plan_upload_list(ctlab_plan *p, const int *h_views, int n, cudaStream_t s);
+int plan_check_device_error(ctlab_plan *p, cudaStream_t s);
+void timing_mark(ctlab_plan *p, int which, cudaStream_t s);
+
+} // namespace ctlab

@@ -1,0 +1,227 @@
+// Device-resident OS-SART and FISTA-TV drivers.
+//
+// Everything stays on the device for the whole solve; per subset step the
+// library launches: volume SAT(s) of x, the projector with the SART
+// residual weighting fused into its epilogue, the projection SAT of the
+// weighted residual, and the backprojector with the OS-SART voxel update
+// fused into its epilogue.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "plan.h"
+
+using namespace ctlab;
+
+namespace {
+
+struct DevBuf {
+    void *p = nullptr;
+    ~DevBuf()
+    {
+        if (p) cudaFree(p);
+    }
+    template <class T>
+    T *as()
+    {
+        return (T *)p;
+    }
+};
+
+int alloc(DevBuf &b, size_t bytes)
+{
+    cudaError_t e = cudaMalloc(&b.p, bytes ? bytes : 1);
+    if (e != cudaSuccess) return cuda_status(e, "reconstruction workspace");
+    return CTLAB_OK;
+}
+
+// ||b - A x|| / ||b|| for the current x over the views of d_order (all PN).
+int exact_residual(ctlab_plan *p, const float *d_x, const unsigned char *d_mask, const int *d_order,
+                   const float *d_bsub, float *d_est, double *d_acc, cudaStream_t s, float *out)
+{
+    const HostGeometry &g = p->g;
+    const long long nd = (long long)g.DNU * g.DNV;
+    int rc = plan_volume_sat(p, d_x, d_mask, s);
+    if (rc != CTLAB_OK) return rc;
+    rc = plan_proj_list(p, d_order, g.PN, d_est, s, PROJ_PLAIN, nullptr, nullptr, nullptr);
+    if (rc != CTLAB_OK) return rc;
+    CTLAB_CUDA_TRY(cudaMemsetAsync(d_acc, 0, 2 * sizeof(double), s));
+    CTLAB_CUDA_TRY(launch_resid2(d_bsub, d_est, nd * g.PN, d_acc, s));
+    double h[2];
+    CTLAB_CUDA_TRY(cudaMemcpyAsync(h, d_acc, sizeof h, cudaMemcpyDeviceToHost, s));
+    CTLAB_CUDA_TRY(cudaStreamSynchronize(s));
+    *out = (float)(h[1] > 0 ? std::sqrt(h[0] / h[1]) : 0.0);
+    return CTLAB_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int ctlab_os_sart(ctlab_plan *plan, float *d_x, const float *d_meas, const unsigned char *d_mask, int os_num,
+                  int iter_num, float lambda, const int *h_order, int clamp, float min_v, float max_v,
+                  float *h_resid, void *stream)
+{
+    if (!plan || !d_x || !d_meas) return set_status(CTLAB_ERR_INVALID_ARG, "null plan, image or projection");
+    if (os_num < 1 || iter_num < 0) return set_status(CTLAB_ERR_INVALID_ARG, "os_num must be >= 1, iter_num >= 0");
+    const HostGeometry &g = plan->g;
+    if (os_num > g.PN) return set_status(CTLAB_ERR_INVALID_ARG, "more subsets than views");
+    if (!g.flat_uniform || plan->q_capacity == 0)
+        return set_status(CTLAB_ERR_UNSUPPORTED, "OS-SART needs a flat detector with uniform u and v pitch");
+    std::lock_guard<std::mutex> lk(plan->mu);
+    DeviceGuard dg(plan->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    plan->last_launches = 0;
+
+    // subset-major view order and subset extents
+    std::vector<int> order(g.PN), off(os_num + 1, 0);
+    if (h_order) {
+        std::vector<char> seen(g.PN, 0);
+        for (int i = 0; i < g.PN; ++i) {
+            const int v = h_order[i];
+            if (v < 0 || v >= g.PN || seen[v])
+                return set_status(CTLAB_ERR_INVALID_ARG, "h_order is not a permutation of 0..PN-1");
+            seen[v] = 1;
+            order[i] = v;
+        }
+        const int per = (g.PN + os_num - 1) / os_num;
+        for (int k = 0; k <= os_num; ++k) off[k] = std::min(g.PN, k * per);
+    } else {
+        int pos = 0;
+        for (int k = 0; k < os_num; ++k) {
+            off[k] = pos;
+            for (int v = k; v < g.PN; v += os_num) order[pos++] = v;
+        }
+        off[os_num] = pos;
+    }
+    int nmax = 0;
+    for (int k = 0; k < os_num; ++k) nmax = std::max(nmax, off[k + 1] - off[k]);
+
+    const long long nd = (long long)g.DNU * g.DNV;
+    const long long nv = (long long)g.XN * g.YN * g.ZN;
+    DevBuf d_order, d_bsub, d_rows, d_cols, d_r, d_ones, d_acc, d_est;
+    int rc = alloc(d_order, sizeof(int) * g.PN);
+    if (rc == CTLAB_OK) rc = alloc(d_bsub, sizeof(float) * nd * g.PN);
+    if (rc == CTLAB_OK) rc = alloc(d_rows, sizeof(float) * nd * g.PN);
+    if (rc == CTLAB_OK) rc = alloc(d_cols, sizeof(float) * nv * os_num);
+    if (rc == CTLAB_OK) rc = alloc(d_r, sizeof(float) * nd * nmax);
+    if (rc == CTLAB_OK) rc = alloc(d_ones, sizeof(float) * std::max(nd * nmax, nv));
+    if (rc == CTLAB_OK) rc = alloc(d_acc, sizeof(double) * 2);
+    if (rc == CTLAB_OK && h_resid) rc = alloc(d_est, sizeof(float) * nd * g.PN);
+    if (rc != CTLAB_OK) return rc;
+    CTLAB_CUDA_TRY(cudaMemcpyAsync(d_order.p, order.data(), sizeof(int) * g.PN, cudaMemcpyHostToDevice, s));
+    CTLAB_CUDA_TRY(launch_gather_views(d_meas, d_order.as<int>(), g.PN, nd, d_bsub.as<float>(), s));
+
+    // rowSum = A 1 (masked volume of ones), colSum_s = B_s 1
+    CTLAB_CUDA_TRY(launch_fill(d_ones.as<float>(), 1.f, std::max(nd * nmax, nv), s));
+    rc = plan_volume_sat(plan, d_ones.as<float>(), d_mask, s);
+    if (rc == CTLAB_OK)
+        rc = plan_proj_list(plan, d_order.as<int>(), g.PN, d_rows.as<float>(), s, PROJ_PLAIN, nullptr, nullptr,
+                            nullptr);
+    for (int k = 0; k < os_num && rc == CTLAB_OK; ++k) {
+        const int n = off[k + 1] - off[k];
+        const int *lst = d_order.as<int>() + off[k];
+        rc = plan_proj_sat(plan, lst, n, d_ones.as<float>(), s);
+        if (rc == CTLAB_OK)
+            rc = plan_back_list(plan, lst, n, d_mask, d_cols.as<float>() + nv * k, s, BACK_PLAIN, nullptr, 1.f, 0,
+                                0.f, 0.f);
+    }
+    if (rc != CTLAB_OK) return rc;
+
+    for (int it = 0; it < iter_num; ++it) {
+        for (int k = 0; k < os_num; ++k) {
+            const int n = off[k + 1] - off[k];
+            if (n == 0) continue;
+            const int *lst = d_order.as<int>() + off[k];
+            rc = plan_volume_sat(plan, d_x, d_mask, s);
+            if (rc == CTLAB_OK)
+                rc = plan_proj_list(plan, lst, n, d_r.as<float>(), s, PROJ_SART_RESIDUAL,
+                                    d_bsub.as<float>() + nd * off[k], d_rows.as<float>() + nd * off[k], nullptr);
+            if (rc == CTLAB_OK) rc = plan_proj_sat(plan, lst, n, d_r.as<float>(), s);
+            if (rc == CTLAB_OK)
+                rc = plan_back_list(plan, lst, n, d_mask, d_x, s, BACK_SART_UPDATE, d_cols.as<float>() + nv * k,
+                                    lambda, clamp, min_v, max_v);
+            if (rc != CTLAB_OK) return rc;
+        }
+        if (h_resid) {
+            rc = exact_residual(plan, d_x, d_mask, d_order.as<int>(), d_bsub.as<float>(), d_est.as<float>(),
+                                d_acc.as<double>(), s, h_resid + it);
+            if (rc != CTLAB_OK) return rc;
+        }
+    }
+    rc = plan_check_device_error(plan, s);
+    return rc == CTLAB_OK ? ok() : rc;
+}
+
+int ctlab_fista_tv(ctlab_plan *plan, float *d_x, const float *d_meas, const unsigned char *d_mask, int iter_num,
+                   float tv_lambda, float tv_eps, float min_v, float max_v, float *h_resid, void *stream)
+{
+    if (!plan || !d_x || !d_meas) return set_status(CTLAB_ERR_INVALID_ARG, "null plan, image or projection");
+    if (iter_num < 0 || !(tv_eps >= 0)) return set_status(CTLAB_ERR_INVALID_ARG, "bad FISTA-TV arguments");
+    const HostGeometry &g = plan->g;
+    if (!g.flat_uniform || plan->q_capacity == 0)
+        return set_status(CTLAB_ERR_UNSUPPORTED, "FISTA-TV needs a flat detector with uniform u and v pitch");
+    std::lock_guard<std::mutex> lk(plan->mu);
+    DeviceGuard dg(plan->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    plan->last_launches = 0;
+    const long long nd = (long long)g.DNU * g.DNV * g.PN;
+    const long long nv = (long long)g.XN * g.YN * g.ZN;
+    const int *all = plan->d_all_views;
+
+    DevBuf d_rows, d_cols, d_r, d_ones, d_y, d_xk, d_xp, d_g, d_acc, d_est;
+    int rc = alloc(d_rows, sizeof(float) * nd);
+    if (rc == CTLAB_OK) rc = alloc(d_cols, sizeof(float) * nv);
+    if (rc == CTLAB_OK) rc = alloc(d_r, sizeof(float) * nd);
+    if (rc == CTLAB_OK) rc = alloc(d_ones, sizeof(float) * std::max(nd, nv));
+    if (rc == CTLAB_OK) rc = alloc(d_y, sizeof(float) * nv);
+    if (rc == CTLAB_OK) rc = alloc(d_xk, sizeof(float) * nv);
+    if (rc == CTLAB_OK) rc = alloc(d_xp, sizeof(float) * nv);
+    if (rc == CTLAB_OK) rc = alloc(d_g, sizeof(float) * nv);
+    if (rc == CTLAB_OK) rc = alloc(d_acc, sizeof(double) * 2);
+    if (rc == CTLAB_OK && h_resid) rc = alloc(d_est, sizeof(float) * nd);
+    if (rc != CTLAB_OK) return rc;
+
+    CTLAB_CUDA_TRY(launch_fill(d_ones.as<float>(), 1.f, std::max(nd, nv), s));
+    rc = plan_volume_sat(plan, d_ones.as<float>(), d_mask, s);
+    if (rc == CTLAB_OK)
+        rc = plan_proj_list(plan, all, g.PN, d_rows.as<float>(), s, PROJ_PLAIN, nullptr, nullptr, nullptr);
+    if (rc == CTLAB_OK) rc = plan_proj_sat(plan, all, g.PN, d_ones.as<float>(), s);
+    if (rc == CTLAB_OK)
+        rc = plan_back_list(plan, all, g.PN, d_mask, d_cols.as<float>(), s, BACK_PLAIN, nullptr, 1.f, 0, 0.f, 0.f);
+    if (rc != CTLAB_OK) return rc;
+    CTLAB_CUDA_TRY(cudaMemcpyAsync(d_y.p, d_x, sizeof(float) * nv, cudaMemcpyDeviceToDevice, s));
+    CTLAB_CUDA_TRY(cudaMemcpyAsync(d_xp.p, d_x, sizeof(float) * nv, cudaMemcpyDeviceToDevice, s));
+
+    float t = 1.f;
+    float *xk = d_xk.as<float>(), *xp = d_xp.as<float>(), *y = d_y.as<float>();
+    for (int it = 0; it < iter_num; ++it) {
+        rc = plan_volume_sat(plan, y, d_mask, s);
+        if (rc == CTLAB_OK)
+            rc = plan_proj_list(plan, all, g.PN, d_r.as<float>(), s, PROJ_SART_RESIDUAL, d_meas, d_rows.as<float>(),
+                                nullptr);
+        if (rc == CTLAB_OK) rc = plan_proj_sat(plan, all, g.PN, d_r.as<float>(), s);
+        // z = (y + B r / colSum) * mask, in place in y
+        if (rc == CTLAB_OK)
+            rc = plan_back_list(plan, all, g.PN, d_mask, y, s, BACK_SART_UPDATE, d_cols.as<float>(), 1.f, 0, 0.f,
+                                0.f);
+        if (rc != CTLAB_OK) return rc;
+        CTLAB_CUDA_TRY(launch_tv_gradient(y, d_g.as<float>(), g.XN, g.YN, g.ZN, tv_eps, s));
+        CTLAB_CUDA_TRY(launch_tv_step(xk, y, d_g.as<float>(), d_mask, tv_lambda, nv, g.ZN, s));
+        const float tn = 0.5f * (1.f + std::sqrt(1.f + 4.f * t * t));
+        CTLAB_CUDA_TRY(cudaMemcpyAsync(y, xk, sizeof(float) * nv, cudaMemcpyDeviceToDevice, s));
+        CTLAB_CUDA_TRY(launch_fista_step(xp, y, t, tn, nv, min_v, max_v, s));
+        plan->last_launches += 3;
+        std::swap(xk, xp); // xp now holds x_k
+        t = tn;
+        if (h_resid) {
+            rc = exact_residual(plan, xp, d_mask, all, d_meas, d_est.as<float>(), d_acc.as<double>(), s, h_resid + it);
+            if (rc != CTLAB_OK) return rc;
+        }
+    }
+    CTLAB_CUDA_TRY(cudaMemcpyAsync(d_x, xp, sizeof(float) * nv, cudaMemcpyDeviceToDevice, s));
+    rc = plan_check_device_error(plan, s);
+    return rc == CTLAB_OK ? ok() : rc;
+}
+
+} // extern "C"

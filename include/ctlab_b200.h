@@ -1,0 +1,237 @@
+/*
+ * ctlab_b200.h -- C ABI of libctlab_b200.so, a B200 (sm_100a) implementation
+ * of CTLAB's branchless distance-driven (DD3) cone-beam projector,
+ * backprojector and the OS-SART / FISTA-TV loops that drive them.
+ *
+ * Data conventions (identical for every entry point):
+ *   volume   float[XN*YN*ZN] in (Z,X,Y) order, z fastest:
+ *              vol[(y*XN + x)*ZN + z]
+ *   mask     unsigned char[XN*YN], mask[y*XN + x] != 0 keeps the voxel
+ *            column; applied to every z.  NULL means "all ones".
+ *   proj     float[PN*DNU*DNV] in [view][u][v] order, v fastest.
+ *   geometry the source starts at (x0,y0,z0), detector cell centres at
+ *            (xds[u], yds[u], zds[v]); view p rotates both by
+ *            theta = hangs[p] (radians, regularised to [0,2pi)) about z and
+ *            shifts z by hzPos[p].  Voxel (x,y,z) is centred at
+ *            (imgXCenter + (x-(XN-1)/2)*dx, imgYCenter + (y-(YN-1)/2)*dx,
+ *             imgZCenter + (z-(ZN-1)/2)*dz).  Lengths in one unit (mm).
+ *   backprojection and the reconstruction loops need a flat detector with
+ *            uniform pitch in u and in v; projection takes any detector.
+ *
+ * Errors: every int-returning entry point returns CTLAB_OK (0) or one of the
+ * CTLAB_ERR_* codes and records a message readable with ctlab_last_error()
+ * on the calling thread.  The void entry points kept from the reference
+ * record the status the same way (read it with ctlab_last_status()).  The
+ * library never exits the process.
+ */
+#ifndef CTLAB_B200_H_
+#define CTLAB_B200_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CTLAB_OK 0
+#define CTLAB_ERR_INVALID_ARG 1
+#define CTLAB_ERR_UNSUPPORTED 2
+#define CTLAB_ERR_CUDA 3
+#define CTLAB_ERR_OOM 4
+#define CTLAB_ERR_TIMEOUT 5
+#define CTLAB_ERR_INTERNAL 6
+
+/* Projection / backprojection models (ForwardDDMethod / BackwardDDMethod,
+ * src/utilities.cuh:853-854; prjMode values of src/DD3_GPU_Proj.h:40 and
+ * src/DD3_GPU_Back.h:39).  Only the branchless model (0) is implemented;
+ * any other value returns CTLAB_ERR_UNSUPPORTED. */
+#define CTLAB_PROJ_BRANCHLESS 0
+#define CTLAB_BACK_BRANCHLESS 0
+
+/* Summed-area-table arithmetic: FP64 prefix sums, or compensated FP32 pairs
+ * (hi+lo float-float sums).  Both store 8 bytes per entry. */
+#define CTLAB_SAT_FP64 0
+#define CTLAB_SAT_F32PAIR 1
+
+/* ---------------------------------------------------------------------- */
+/* Entry points with the reference's names and argument order             */
+/* ---------------------------------------------------------------------- */
+
+/* Branchless DD forward projection of the host volume hvol into the host
+ * projection hprj on GPU gpunum.  Replaces DD3Proj_gpu,
+ * src/DD3_GPU_Proj.h:41-44 (same name, arguments and order). */
+void DD3Proj_gpu(float x0, float y0, float z0, int DNU, int DNV, float *xds, float *yds,
+                 float *zds, float imgXCenter, float imgYCenter, float imgZCenter,
+                 float *hangs, float *hzPos, int PN, int XN, int YN, int ZN, float *hvol,
+                 float *hprj, float dx, float dz, unsigned char *mask, int gpunum, int prjMode);
+
+/* Branchless DD backprojection of the host projection hprj into the host
+ * volume hvol on GPU gpunum; `squared` is ignored, as documented by the
+ * reference.  Replaces DD3Back_gpu, src/DD3_GPU_Back.h:40-44. */
+void DD3Back_gpu(float x0, float y0, float z0, int DNU, int DNV, float *xds, float *yds,
+                 float *zds, float imgXCenter, float imgYCenter, float imgZCenter,
+                 float *hangs, float *hzPos, int PN, int XN, int YN, int ZN, float *hvol,
+                 float *hprj, float dx, float dz, unsigned char *mask, int gpunum,
+                 int squared, int prjMode);
+
+/* Status of the last call on this thread (CTLAB_OK or CTLAB_ERR_*), and its
+ * message ("" after success).  New in this library: the reference ignores
+ * CUDA errors or exits (src/utilities.cuh:63-76). */
+int ctlab_last_status(void);
+const char *ctlab_last_error(void);
+
+/* ---------------------------------------------------------------------- */
+/* Plans: device-resident geometry, workspaces and stream-ordered calls     */
+/* ---------------------------------------------------------------------- */
+
+/* Geometry of one scan.  Pointers are HOST arrays read during
+ * ctlab_plan_create only: xds, yds [DNU]; zds [DNV]; hangs, hzPos [PN].
+ * Mirrors the scalar and array arguments of DD3Proj_gpu. */
+typedef struct ctlab_geometry {
+    float x0, y0, z0;
+    int DNU, DNV;
+    const float *xds;
+    const float *yds;
+    const float *zds;
+    float imgXCenter, imgYCenter, imgZCenter;
+    const float *hangs;
+    const float *hzPos;
+    int PN;
+    int XN, YN, ZN;
+    float dx, dz;
+} ctlab_geometry;
+
+typedef struct ctlab_plan ctlab_plan;
+
+/* Validates the geometry, uploads per-view constants and allocates the SAT
+ * workspaces on `device`.  sat_mode is CTLAB_SAT_FP64 or
+ * CTLAB_SAT_F32PAIR.  The plan is used from one stream at a time.
+ * New in this library (the reference recomputes everything per call). */
+int ctlab_plan_create(const ctlab_geometry *geom, int device, int sat_mode, ctlab_plan **out);
+int ctlab_plan_destroy(ctlab_plan *plan);
+/* Device bytes held by the plan. */
+long long ctlab_plan_workspace_bytes(const ctlab_plan *plan);
+
+/* Forward projection of the device volume d_vol (masked by d_mask, may be
+ * NULL) into d_prj[PN][DNU][DNV], stream-ordered on `stream`
+ * (a cudaStream_t; NULL = legacy default stream).  Device pointers are owned
+ * by the caller.  The device-pointer form of DD3Proj_gpu. */
+int ctlab_proj(ctlab_plan *plan, const float *d_vol, const unsigned char *d_mask, float *d_prj,
+               void *stream);
+
+/* Forward projection of the views listed in h_views[n] (host indices into
+ * the plan's views) into d_prj[n][DNU][DNV]. */
+int ctlab_proj_views(ctlab_plan *plan, const int *h_views, int n, const float *d_vol,
+                     const unsigned char *d_mask, float *d_prj, void *stream);
+
+/* Backprojection of d_prj[PN][DNU][DNV] into d_vol (overwritten), masked by
+ * d_mask.  The device-pointer form of DD3Back_gpu. */
+int ctlab_back(ctlab_plan *plan, const float *d_prj, const unsigned char *d_mask, float *d_vol,
+               void *stream);
+
+/* Backprojection of d_prj[n][DNU][DNV] holding the views h_views[n]. */
+int ctlab_back_views(ctlab_plan *plan, const int *h_views, int n, const float *d_prj,
+                     const unsigned char *d_mask, float *d_vol, void *stream);
+
+/* Builds the two volume SATs of the masked volume into the plan's
+ * workspace (the first step of ctlab_proj), for tests and timing. */
+int ctlab_volume_sat(ctlab_plan *plan, const float *d_vol, const unsigned char *d_mask,
+                     void *stream);
+
+/* Copies the plan's volume SAT of one orientation to d_out (FP64 plans:
+ * doubles, [planes][rows][zp] as reported by ctlab_plan_sat_layout;
+ * F32PAIR plans: float pairs (hi, lo) with the same indexing). */
+int ctlab_plan_sat_layout(const ctlab_plan *plan, int orientation, int *planes, int *rows,
+                          int *zp);
+int ctlab_copy_volume_sat(ctlab_plan *plan, int orientation, void *d_out, void *stream);
+
+/* Elapsed device milliseconds of the last ctlab_proj / ctlab_back call
+ * split into SAT build and gather kernels (measured with CUDA events on the
+ * launching stream when timing is enabled with ctlab_plan_set_timing). */
+int ctlab_plan_set_timing(ctlab_plan *plan, int enable);
+int ctlab_plan_last_times(ctlab_plan *plan, float *sat_ms, float *gather_ms);
+
+/* Number of the library's kernels launched by the last ctlab_proj /
+ * ctlab_back / reconstruction call on this plan. */
+int ctlab_plan_last_launches(const ctlab_plan *plan);
+
+/* ---------------------------------------------------------------------- */
+/* Reconstruction                                                          */
+/* ---------------------------------------------------------------------- */
+
+/* OS-SART on the device.  d_x holds the initial image and receives the
+ * result; d_meas is the measured projection [PN][DNU][DNV].  Views are split
+ * into os_num interleaved subsets {s, s+os_num, ...} unless h_order[PN] (a
+ * permutation of 0..PN-1, may be NULL) gives the subset-major view order,
+ * subset s taking positions [s*ceil(PN/os_num), ...).  Each subset step:
+ *   r = (b_s - A_s x)/rowSum_s   (0 where rowSum_s <= 1e-7)
+ *   x = (x + lambda * (B_s r)/colSum_s) * mask  (0 where colSum_s <= 1e-7)
+ * optionally clamped to [min_v, max_v] when clamp != 0.  If h_resid is not
+ * NULL it receives iter_num values ||b - A x_k|| / ||b|| after each
+ * iteration.  Replaces the GPU body of OS_SART, src/DD3_GPU_recon.h:60-65. */
+int ctlab_os_sart(ctlab_plan *plan, float *d_x, const float *d_meas, const unsigned char *d_mask,
+                  int os_num, int iter_num, float lambda, const int *h_order, int clamp,
+                  float min_v, float max_v, float *h_resid, void *stream);
+
+/* FISTA-TV on the device: SART-preconditioned gradient step over all views,
+ * one TV-gradient step of weight tv_lambda (smoothing tv_eps), FISTA
+ * momentum clamped to [min_v, max_v] (FISTA_functor,
+ * src/FastIterativeShrinkageAlgorithm.h:17-42).  h_resid as for
+ * ctlab_os_sart. */
+int ctlab_fista_tv(ctlab_plan *plan, float *d_x, const float *d_meas,
+                   const unsigned char *d_mask, int iter_num, float tv_lambda, float tv_eps,
+                   float min_v, float max_v, float *h_resid, void *stream);
+
+/* Smoothed isotropic TV gradient of d_f into d_g (both (Z,X,Y)).  The 3-D
+ * form of GradientOfTV_GPU, src/differentialFuncs.hpp:491-501. */
+int ctlab_tv_gradient(const float *d_f, float *d_g, int XN, int YN, int ZN, float eps,
+                      void *stream);
+
+/* FISTA momentum step on device arrays: cur = clamp(cur + (t1-1)/t2 (cur -
+ * las), minV, maxV).  FISTA, src/FastIterativeShrinkageAlgorithm.h:44-48. */
+int ctlab_fista_step(const float *d_las, float *d_cur, float t1, float t2, long long n,
+                     float min_v, float max_v, void *stream);
+
+/* SART weightings on device arrays, epsilon 1e-7:
+ *   prj = rowSum > eps ? (real - prj)/rowSum : 0
+ *   vol = colSum > eps ? vol/colSum : 0;  recon += vol
+ * SART_Weighting::Proj_ptr / Back_ptr, src/SARTWeighting.h:38-91. */
+int ctlab_sart_proj_weight(float *d_prj, const float *d_real, const float *d_row_sum, long long n,
+                           void *stream);
+int ctlab_sart_back_weight(float *d_vol, float *d_recon, const float *d_col_sum, long long n,
+                           void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* Phantoms (test and benchmark inputs)                                    */
+/* ---------------------------------------------------------------------- */
+
+/* Point-sampled sum of rotated ellipsoids at voxel centres into d_vol.
+ * h_ell holds n_ell records of 10 floats: value, cx, cy, cz, ax, ay, az
+ * (semi-axes), phi, theta, psi (R = Rz(phi) Rx(theta) Rz(psi)). */
+int ctlab_ellipsoid_phantom(float *d_vol, int XN, int YN, int ZN, float dx, float dz,
+                            float imgXCenter, float imgYCenter, float imgZCenter,
+                            const double *h_ell, int n_ell, int clamp_nonneg, void *stream);
+
+/* Random-ellipsoid parameters drawn with std::mt19937_64(seed): count
+ * uniform in [n_min, n_max], centres uniform in 0.8 x the half extents,
+ * semi-axes U(0.05,0.4) x half extent per axis, Euler angles U(0,pi),
+ * values U(0, v_max).  Writes up to cap records into h_ell, returns the
+ * count (or a negative CTLAB_ERR_* value). */
+int ctlab_random_ellipsoids(unsigned long long seed, int n_min, int n_max, float half_x,
+                            float half_y, float half_z, float v_max, double *h_ell, int cap);
+
+/* ---------------------------------------------------------------------- */
+/* Diagnostics                                                             */
+/* ---------------------------------------------------------------------- */
+
+/* Runs a two-chunk SAT scan on `device` whose first chunk never publishes
+ * its result, so the second chunk's bounded wait (spin_limit polls of about
+ * 64 ns) runs out.  Returns CTLAB_ERR_TIMEOUT when the timeout was detected
+ * and reported through the device error word as designed (the launch
+ * terminates and the context stays usable), CTLAB_ERR_INTERNAL otherwise.
+ * No counterpart in the reference, which has no device-side waits. */
+int ctlab_debug_scan_stall(int device, unsigned spin_limit);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CTLAB_B200_H_ */
