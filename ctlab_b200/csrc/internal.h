@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -155,10 +156,22 @@ struct ProjArgs {
     int epilogue;
     const float *meas;    // [n][DNU][DNV]  (SART residual)
     const float *row_sum; // [n][DNU][DNV]
-    double *resid2;       // accumulates sum (meas - Ax)^2 and sum meas^2
+    double *resid2;       // accumulates sum (meas - Ax)^2
+    int cmax;             // staging-buffer columns (proj_staging_columns)
+    int *err;             // device error word (bounded waits)
+    const int *groups;    // [ngroups][G] list positions sharing a CTA (-1: empty)
+    int ngroups, G;
 };
+
+// Views of one launch grouped by driving axis and angle, G per CTA.
+struct ProjGroups {
+    std::vector<int> table; // [ngroups][G] list positions, -1 pads a partial group
+    int ngroups = 0, G = 1;
+};
+ProjGroups proj_make_groups(const HostGeometry &g, const std::vector<int> &list, int cmax);
 cudaError_t launch_proj(const ProjArgs &a, cudaStream_t s, int *launches);
 bool proj_supported(int ZN, int DNV);
+int proj_staging_columns(const HostGeometry &g, int zp);
 
 enum BackEpilogue { BACK_PLAIN = 0, BACK_SART_UPDATE = 1 };
 
@@ -181,9 +194,12 @@ struct BackArgs {
     float lambda;
     int clamp;
     float min_v, max_v;
+    int rmax;             // staging-buffer SAT rows (back_staging_rows)
+    int *err;             // device error word (bounded waits)
 };
 cudaError_t launch_back(const BackArgs &a, cudaStream_t s, int *launches);
 bool back_supported(int DNV);
+int back_staging_rows(const HostGeometry &g, int vp);
 
 // elementwise
 cudaError_t launch_sart_proj_weight(float *prj, const float *real, const float *row_sum, long long n,

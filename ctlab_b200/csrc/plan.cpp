@@ -36,7 +36,8 @@ void plan_free(ctlab_plan *p)
     if (!p) return;
     DeviceGuard g(p->device);
     void *bufs[] = {p->d_views, p->d_det, p->d_all_views, p->d_list, p->d_sat_y, p->d_sat_x,
-                    p->d_q, p->d_ticket, p->d_flags, p->d_agg, p->d_pref, p->d_err};
+                    p->d_q, p->d_ticket, p->d_flags, p->d_agg, p->d_pref, p->d_err,
+                    p->d_groups_all, p->d_groups_scratch};
     for (void *b : bufs)
         if (b) cudaFree(b);
     for (auto &e : p->ev)
@@ -63,8 +64,25 @@ int plan_volume_sat(ctlab_plan *p, const float *d_vol, const unsigned char *d_ma
     return CTLAB_OK;
 }
 
-int plan_proj_list(ctlab_plan *p, const int *d_list, int n, float *d_prj, cudaStream_t s, int epilogue,
-                   const float *meas, const float *row_sum, double *resid2)
+int plan_groups(ctlab_plan *p, const std::vector<int> &host_list, int *d_dst, int cap, GroupTab &out,
+                cudaStream_t s)
+{
+    std::vector<int> ids(host_list.size());
+    for (size_t i = 0; i < host_list.size(); ++i) ids[i] = host_list[i];
+    ProjGroups pg = proj_make_groups(p->g, ids, p->proj_cmax);
+    if ((int)pg.table.size() > cap) return set_status(CTLAB_ERR_INTERNAL, "group table capacity exceeded");
+    if (!pg.table.empty()) {
+        CTLAB_CUDA_TRY(cudaMemcpyAsync(d_dst, pg.table.data(), sizeof(int) * pg.table.size(), cudaMemcpyHostToDevice, s));
+        CTLAB_CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    out.d = d_dst;
+    out.ngroups = pg.ngroups;
+    out.G = pg.G;
+    return CTLAB_OK;
+}
+
+int plan_proj_list(ctlab_plan *p, const int *d_list, int n, const GroupTab &gt, float *d_prj, cudaStream_t s,
+                   int epilogue, const float *meas, const float *row_sum, double *resid2)
 {
     const HostGeometry &g = p->g;
     ProjArgs a;
@@ -85,6 +103,11 @@ int plan_proj_list(ctlab_plan *p, const int *d_list, int n, float *d_prj, cudaSt
     a.meas = meas;
     a.row_sum = row_sum;
     a.resid2 = resid2;
+    a.cmax = p->proj_cmax;
+    a.err = p->d_err;
+    a.groups = gt.d;
+    a.ngroups = gt.ngroups;
+    a.G = gt.G;
     cudaError_t e = launch_proj(a, s, &p->last_launches);
     if (e != cudaSuccess) return cuda_status(e, "DD3 projection kernel");
     return CTLAB_OK;
@@ -141,6 +164,8 @@ int plan_back_list(ctlab_plan *p, const int *d_list, int n, const unsigned char 
     a.clamp = clamp;
     a.min_v = min_v;
     a.max_v = max_v;
+    a.rmax = p->back_rmax;
+    a.err = p->d_err;
     if (n == 0 && epilogue == BACK_PLAIN) {
         CTLAB_CUDA_TRY(cudaMemsetAsync(d_vol, 0, sizeof(float) * (size_t)g.XN * g.YN * g.ZN, s));
         return CTLAB_OK;
@@ -222,6 +247,8 @@ int ctlab_plan_create(const ctlab_geometry *geom, int device, int sat_mode, ctla
     p->zp = round_up(g.ZN + 1, 2);
     p->vp = round_up(g.DNV + 1, 2);
     p->q_capacity = g.PN;
+    p->proj_cmax = proj_staging_columns(g, p->zp);
+    if (g.flat_uniform) p->back_rmax = back_staging_rows(g, p->vp);
 
     long long &bytes = p->bytes;
     cudaError_t e = cudaSuccess;
@@ -255,6 +282,9 @@ int ctlab_plan_create(const ctlab_geometry *geom, int device, int sat_mode, ctla
     chk(dmalloc(&p->d_agg, state, bytes));
     chk(dmalloc(&p->d_pref, state, bytes));
     chk(dmalloc(&p->d_err, 1, bytes));
+    p->groups_cap = 2 * g.PN + 16;
+    chk(dmalloc(&p->d_groups_all, (size_t)p->groups_cap, bytes));
+    chk(dmalloc(&p->d_groups_scratch, (size_t)p->groups_cap, bytes));
     if (e != cudaSuccess) {
         plan_free(p);
         return cuda_status(e, "plan workspace allocation");
@@ -269,6 +299,16 @@ int ctlab_plan_create(const ctlab_geometry *geom, int device, int sat_mode, ctla
     if (e != cudaSuccess) {
         plan_free(p);
         return cuda_status(e, "plan upload");
+    }
+    {
+        GroupTab gt;
+        int grc = plan_groups(p, all, p->d_groups_all, p->groups_cap, gt, 0);
+        if (grc != CTLAB_OK) {
+            plan_free(p);
+            return grc;
+        }
+        p->groups_all_n = gt.ngroups;
+        p->groups_all_G = gt.G;
     }
     *out = p;
     return ok();
@@ -350,7 +390,8 @@ int ctlab_proj(ctlab_plan *plan, const float *d_vol, const unsigned char *d_mask
     int rc = plan_volume_sat(plan, d_vol, d_mask, s);
     if (rc != CTLAB_OK) return rc;
     timing_mark(plan, 1, s);
-    rc = plan_proj_list(plan, plan->d_all_views, plan->g.PN, d_prj, s, PROJ_PLAIN, nullptr, nullptr, nullptr);
+    rc = plan_proj_list(plan, plan->d_all_views, plan->g.PN, plan_all_groups(plan), d_prj, s, PROJ_PLAIN, nullptr,
+                        nullptr, nullptr);
     if (rc != CTLAB_OK) return rc;
     timing_mark(plan, 2, s);
     return ok();
@@ -367,11 +408,16 @@ int ctlab_proj_views(ctlab_plan *plan, const int *h_views, int n, const float *d
     int rc = plan_upload_list(plan, h_views, n, s);
     if (rc != CTLAB_OK) return rc;
     if (n == 0) return ok();
+    std::vector<int> positions(n);
+    for (int i = 0; i < n; ++i) positions[i] = h_views[i];
+    GroupTab gt;
+    rc = plan_groups(plan, positions, plan->d_groups_scratch, plan->groups_cap, gt, s);
+    if (rc != CTLAB_OK) return rc;
     timing_mark(plan, 0, s);
     rc = plan_volume_sat(plan, d_vol, d_mask, s);
     if (rc != CTLAB_OK) return rc;
     timing_mark(plan, 1, s);
-    rc = plan_proj_list(plan, plan->d_list, n, d_prj, s, PROJ_PLAIN, nullptr, nullptr, nullptr);
+    rc = plan_proj_list(plan, plan->d_list, n, gt, d_prj, s, PROJ_PLAIN, nullptr, nullptr, nullptr);
     if (rc != CTLAB_OK) return rc;
     timing_mark(plan, 2, s);
     return ok();

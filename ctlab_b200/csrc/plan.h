@@ -21,6 +21,12 @@ struct ctlab_plan {
     void *d_q = nullptr; // projection SATs [q_capacity][DNU+1][vp]
     int vp = 0;
     int q_capacity = 0;
+    int proj_cmax = 2;  // projector staging columns
+    int *d_groups_all = nullptr;     // projector view groups of the full view list
+    int groups_all_n = 0, groups_all_G = 1;
+    int *d_groups_scratch = nullptr; // groups of a caller's view list
+    int groups_cap = 0;
+    int back_rmax = 2;  // backprojector staging rows
     int *d_ticket = nullptr, *d_flags = nullptr, *d_err = nullptr;
     double *d_agg = nullptr, *d_pref = nullptr;
     bool timing = false;
@@ -32,10 +38,21 @@ struct ctlab_plan {
 
 namespace ctlab {
 
+// Device table of projector view groups (see proj_make_groups).
+struct GroupTab {
+    const int *d = nullptr;
+    int ngroups = 0, G = 1;
+};
+
 void plan_free(ctlab_plan *p);
+// Groups the host list (positions into a device view list) and uploads the
+// table to d_dst (capacity cap ints); synchronous.
+int plan_groups(ctlab_plan *p, const std::vector<int> &host_list, int *d_dst, int cap, GroupTab &out,
+                cudaStream_t s);
+inline GroupTab plan_all_groups(const ctlab_plan *p) { return {p->d_groups_all, p->groups_all_n, p->groups_all_G}; }
 int plan_volume_sat(ctlab_plan *p, const float *d_vol, const unsigned char *d_mask, cudaStream_t s);
-int plan_proj_list(ctlab_plan *p, const int *d_list, int n, float *d_prj, cudaStream_t s, int epilogue,
-                   const float *meas, const float *row_sum, double *resid2);
+int plan_proj_list(ctlab_plan *p, const int *d_list, int n, const GroupTab &gt, float *d_prj, cudaStream_t s,
+                   int epilogue, const float *meas, const float *row_sum, double *resid2);
 int plan_proj_sat(ctlab_plan *p, const int *d_list, int n, const float *d_prj, cudaStream_t s);
 int plan_back_list(ctlab_plan *p, const int *d_list, int n, const unsigned char *d_mask, float *d_vol,
                    cudaStream_t s, int epilogue, const float *col_sum, float lambda, int clamp, float min_v,

@@ -37,13 +37,13 @@ int alloc(DevBuf &b, size_t bytes)
 
 // ||b - A x|| / ||b|| for the current x over the views of d_order (all PN).
 int exact_residual(ctlab_plan *p, const float *d_x, const unsigned char *d_mask, const int *d_order,
-                   const float *d_bsub, float *d_est, double *d_acc, cudaStream_t s, float *out)
+                   const GroupTab &gt, const float *d_bsub, float *d_est, double *d_acc, cudaStream_t s, float *out)
 {
     const HostGeometry &g = p->g;
     const long long nd = (long long)g.DNU * g.DNV;
     int rc = plan_volume_sat(p, d_x, d_mask, s);
     if (rc != CTLAB_OK) return rc;
-    rc = plan_proj_list(p, d_order, g.PN, d_est, s, PROJ_PLAIN, nullptr, nullptr, nullptr);
+    rc = plan_proj_list(p, d_order, g.PN, gt, d_est, s, PROJ_PLAIN, nullptr, nullptr, nullptr);
     if (rc != CTLAB_OK) return rc;
     CTLAB_CUDA_TRY(cudaMemsetAsync(d_acc, 0, 2 * sizeof(double), s));
     CTLAB_CUDA_TRY(launch_resid2(d_bsub, d_est, nd * g.PN, d_acc, s));
@@ -99,8 +99,10 @@ int ctlab_os_sart(ctlab_plan *plan, float *d_x, const float *d_meas, const unsig
 
     const long long nd = (long long)g.DNU * g.DNV;
     const long long nv = (long long)g.XN * g.YN * g.ZN;
-    DevBuf d_order, d_bsub, d_rows, d_cols, d_r, d_ones, d_acc, d_est;
+    DevBuf d_order, d_bsub, d_rows, d_cols, d_r, d_ones, d_acc, d_est, d_groups;
+    const int gcap = 2 * g.PN + 16;
     int rc = alloc(d_order, sizeof(int) * g.PN);
+    if (rc == CTLAB_OK) rc = alloc(d_groups, sizeof(int) * (size_t)gcap * (os_num + 1));
     if (rc == CTLAB_OK) rc = alloc(d_bsub, sizeof(float) * nd * g.PN);
     if (rc == CTLAB_OK) rc = alloc(d_rows, sizeof(float) * nd * g.PN);
     if (rc == CTLAB_OK) rc = alloc(d_cols, sizeof(float) * nv * os_num);
@@ -111,13 +113,21 @@ int ctlab_os_sart(ctlab_plan *plan, float *d_x, const float *d_meas, const unsig
     if (rc != CTLAB_OK) return rc;
     CTLAB_CUDA_TRY(cudaMemcpyAsync(d_order.p, order.data(), sizeof(int) * g.PN, cudaMemcpyHostToDevice, s));
     CTLAB_CUDA_TRY(launch_gather_views(d_meas, d_order.as<int>(), g.PN, nd, d_bsub.as<float>(), s));
+    // projector view groups: the whole order, then each subset
+    std::vector<GroupTab> gtab(os_num + 1);
+    rc = plan_groups(plan, order, d_groups.as<int>() + (size_t)gcap * os_num, gcap, gtab[os_num], s);
+    for (int k = 0; k < os_num && rc == CTLAB_OK; ++k) {
+        std::vector<int> sub(order.begin() + off[k], order.begin() + off[k + 1]);
+        rc = plan_groups(plan, sub, d_groups.as<int>() + (size_t)gcap * k, gcap, gtab[k], s);
+    }
+    if (rc != CTLAB_OK) return rc;
 
     // rowSum = A 1 (masked volume of ones), colSum_s = B_s 1
     CTLAB_CUDA_TRY(launch_fill(d_ones.as<float>(), 1.f, std::max(nd * nmax, nv), s));
     rc = plan_volume_sat(plan, d_ones.as<float>(), d_mask, s);
     if (rc == CTLAB_OK)
-        rc = plan_proj_list(plan, d_order.as<int>(), g.PN, d_rows.as<float>(), s, PROJ_PLAIN, nullptr, nullptr,
-                            nullptr);
+        rc = plan_proj_list(plan, d_order.as<int>(), g.PN, gtab[os_num], d_rows.as<float>(), s, PROJ_PLAIN, nullptr,
+                            nullptr, nullptr);
     for (int k = 0; k < os_num && rc == CTLAB_OK; ++k) {
         const int n = off[k + 1] - off[k];
         const int *lst = d_order.as<int>() + off[k];
@@ -135,7 +145,7 @@ int ctlab_os_sart(ctlab_plan *plan, float *d_x, const float *d_meas, const unsig
             const int *lst = d_order.as<int>() + off[k];
             rc = plan_volume_sat(plan, d_x, d_mask, s);
             if (rc == CTLAB_OK)
-                rc = plan_proj_list(plan, lst, n, d_r.as<float>(), s, PROJ_SART_RESIDUAL,
+                rc = plan_proj_list(plan, lst, n, gtab[k], d_r.as<float>(), s, PROJ_SART_RESIDUAL,
                                     d_bsub.as<float>() + nd * off[k], d_rows.as<float>() + nd * off[k], nullptr);
             if (rc == CTLAB_OK) rc = plan_proj_sat(plan, lst, n, d_r.as<float>(), s);
             if (rc == CTLAB_OK)
@@ -144,8 +154,8 @@ int ctlab_os_sart(ctlab_plan *plan, float *d_x, const float *d_meas, const unsig
             if (rc != CTLAB_OK) return rc;
         }
         if (h_resid) {
-            rc = exact_residual(plan, d_x, d_mask, d_order.as<int>(), d_bsub.as<float>(), d_est.as<float>(),
-                                d_acc.as<double>(), s, h_resid + it);
+            rc = exact_residual(plan, d_x, d_mask, d_order.as<int>(), gtab[os_num], d_bsub.as<float>(),
+                                d_est.as<float>(), d_acc.as<double>(), s, h_resid + it);
             if (rc != CTLAB_OK) return rc;
         }
     }
@@ -185,7 +195,8 @@ int ctlab_fista_tv(ctlab_plan *plan, float *d_x, const float *d_meas, const unsi
     CTLAB_CUDA_TRY(launch_fill(d_ones.as<float>(), 1.f, std::max(nd, nv), s));
     rc = plan_volume_sat(plan, d_ones.as<float>(), d_mask, s);
     if (rc == CTLAB_OK)
-        rc = plan_proj_list(plan, all, g.PN, d_rows.as<float>(), s, PROJ_PLAIN, nullptr, nullptr, nullptr);
+        rc = plan_proj_list(plan, all, g.PN, plan_all_groups(plan), d_rows.as<float>(), s, PROJ_PLAIN, nullptr, nullptr,
+                            nullptr);
     if (rc == CTLAB_OK) rc = plan_proj_sat(plan, all, g.PN, d_ones.as<float>(), s);
     if (rc == CTLAB_OK)
         rc = plan_back_list(plan, all, g.PN, d_mask, d_cols.as<float>(), s, BACK_PLAIN, nullptr, 1.f, 0, 0.f, 0.f);
@@ -198,8 +209,8 @@ int ctlab_fista_tv(ctlab_plan *plan, float *d_x, const float *d_meas, const unsi
     for (int it = 0; it < iter_num; ++it) {
         rc = plan_volume_sat(plan, y, d_mask, s);
         if (rc == CTLAB_OK)
-            rc = plan_proj_list(plan, all, g.PN, d_r.as<float>(), s, PROJ_SART_RESIDUAL, d_meas, d_rows.as<float>(),
-                                nullptr);
+            rc = plan_proj_list(plan, all, g.PN, plan_all_groups(plan), d_r.as<float>(), s, PROJ_SART_RESIDUAL, d_meas,
+                                d_rows.as<float>(), nullptr);
         if (rc == CTLAB_OK) rc = plan_proj_sat(plan, all, g.PN, d_r.as<float>(), s);
         // z = (y + B r / colSum) * mask, in place in y
         if (rc == CTLAB_OK)
@@ -215,7 +226,8 @@ int ctlab_fista_tv(ctlab_plan *plan, float *d_x, const float *d_meas, const unsi
         std::swap(xk, xp); // xp now holds x_k
         t = tn;
         if (h_resid) {
-            rc = exact_residual(plan, xp, d_mask, all, d_meas, d_est.as<float>(), d_acc.as<double>(), s, h_resid + it);
+            rc = exact_residual(plan, xp, d_mask, all, plan_all_groups(plan), d_meas, d_est.as<float>(),
+                                d_acc.as<double>(), s, h_resid + it);
             if (rc != CTLAB_OK) return rc;
         }
     }

@@ -19,3 +19,12 @@ def cuda_ok():
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
     return True
+
+
+def record_error(name: str, value: float) -> None:
+    """Appends a measured parity error to $CTLAB_PARITY_LOG (JSON lines)."""
+    path = os.environ.get("CTLAB_PARITY_LOG")
+    if path:
+        import json
+        with open(path, "a") as f:
+            f.write(json.dumps({"case": name, "rel_l2": value}) + "\n")

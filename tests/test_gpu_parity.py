@@ -12,6 +12,7 @@ import pytest
 import ctlab_b200 as cb
 import oracle
 from ctlab_b200 import geometry as G
+from conftest import record_error
 
 pytestmark = pytest.mark.gpu
 
@@ -74,6 +75,7 @@ def test_projection_matches_oracle(torch_cuda, name, sat_mode):
         torch.cuda.synchronize()
         got = out.cpu().numpy()
     err = rel_l2(got, ref)
+    record_error(f"proj/{name}/sat{sat_mode}", err)
     assert err <= REL_L2, f"{name}: rel L2 {err:.3e}"
 
 
@@ -92,6 +94,7 @@ def test_backprojection_matches_oracle(torch_cuda, name, sat_mode):
         torch.cuda.synchronize()
         got = out.cpu().numpy()
     err = rel_l2(got, ref)
+    record_error(f"back/{name}/sat{sat_mode}", err)
     assert err <= REL_L2, f"{name}: rel L2 {err:.3e}"
 
 
@@ -133,12 +136,14 @@ def test_config1_views_match_oracle(torch_cuda):
         plan.proj(dev(torch, vol), out)
         torch.cuda.synchronize()
         got = out.cpu().numpy()[views]
+        record_error("proj/config1_36views", rel_l2(got, ref_p))
         assert rel_l2(got, ref_p) <= REL_L2
         prj = got.astype(np.float32)
         ref_b = oracle.dd3_back(gs, prj)
         vb = torch.zeros(g.vol_shape, dtype=torch.float32, device="cuda")
         plan.back_views(views, dev(torch, prj), vb)
         torch.cuda.synchronize()
+        record_error("back/config1_36views", rel_l2(vb.cpu().numpy(), ref_b))
         assert rel_l2(vb.cpu().numpy(), ref_b) <= REL_L2
 
 
@@ -159,11 +164,13 @@ def test_config2_views_match_oracle(torch_cuda):
         plan.proj_views(views, vol, out)
         torch.cuda.synchronize()
         got = out.cpu().numpy()
+        record_error("proj/config2_4views", rel_l2(got, ref_p))
         assert rel_l2(got, ref_p) <= REL_L2
         ref_b = oracle.dd3_back(gs, got)
         vb = torch.zeros(g.vol_shape, dtype=torch.float32, device="cuda")
         plan.back_views(views, out, vb)
         torch.cuda.synchronize()
+        record_error("back/config2_4views", rel_l2(vb.cpu().numpy(), ref_b))
         assert rel_l2(vb.cpu().numpy(), ref_b) <= REL_L2
 
 
@@ -230,6 +237,7 @@ def test_config2_adjointness_full_size(torch_cuda):
         torch.cuda.synchronize()
         a = float((ax.double() * y.double()).sum())
         b = float((x.double() * by.double()).sum())
+    record_error("adjoint_gap/config2", abs(a - b) / abs(a))
     assert abs(a - b) / abs(a) < 1e-4
 
 

@@ -42,12 +42,12 @@ def scan(seed=0):
 def test_sart_weightings_match_reference_golden(torch_cuda):
     torch = torch_cuda
     lib = cb.load()
-    prj = dev(torch, GOLD["sart_prj"])
-    lib.ctlab_sart_proj_weight(prj.data_ptr(), dev(torch, GOLD["sart_real"]).data_ptr(),
-                               dev(torch, GOLD["sart_rs"]).data_ptr(), prj.numel(), None)
+    # keep every device tensor alive until the stream has consumed it
+    prj, real, rs = dev(torch, GOLD["sart_prj"]), dev(torch, GOLD["sart_real"]), dev(torch, GOLD["sart_rs"])
     vol, rec = dev(torch, GOLD["sart_vol"]), dev(torch, GOLD["sart_rec"])
-    lib.ctlab_sart_back_weight(vol.data_ptr(), rec.data_ptr(), dev(torch, GOLD["sart_rs"]).data_ptr(),
-                               vol.numel(), None)
+    torch.cuda.synchronize()
+    lib.ctlab_sart_proj_weight(prj.data_ptr(), real.data_ptr(), rs.data_ptr(), prj.numel(), None)
+    lib.ctlab_sart_back_weight(vol.data_ptr(), rec.data_ptr(), rs.data_ptr(), vol.numel(), None)
     torch.cuda.synchronize()
     np.testing.assert_allclose(prj.cpu().numpy(), GOLD["sart_prj_out"], rtol=1e-6, atol=0)
     np.testing.assert_allclose(vol.cpu().numpy(), GOLD["sart_vol_out"], rtol=1e-6, atol=0)
@@ -58,9 +58,9 @@ def test_fista_step_matches_reference_golden(torch_cuda):
     torch = torch_cuda
     lib = cb.load()
     t1, t2, lo, hi = GOLD["fista_t"]
-    cur = dev(torch, GOLD["fista_cur"])
-    lib.ctlab_fista_step(dev(torch, GOLD["fista_las"]).data_ptr(), cur.data_ptr(), t1, t2, cur.numel(), lo, hi,
-                         None)
+    cur, las = dev(torch, GOLD["fista_cur"]), dev(torch, GOLD["fista_las"])
+    torch.cuda.synchronize()
+    lib.ctlab_fista_step(las.data_ptr(), cur.data_ptr(), t1, t2, cur.numel(), lo, hi, None)
     torch.cuda.synchronize()
     np.testing.assert_allclose(cur.cpu().numpy(), GOLD["fista_out"], rtol=2e-7, atol=1e-3)
 
@@ -72,7 +72,9 @@ def test_tv_gradient_matches_oracle(torch_cuda):
     f = rng.random((YN, XN, ZN)).astype(np.float32)
     ref = oracle.tv_gradient(f, XN, YN, ZN, 1e-8)
     g = torch.zeros((YN, XN, ZN), dtype=torch.float32, device="cuda")
-    cb._lib.check(cb.load().ctlab_tv_gradient(dev(torch, f).data_ptr(), g.data_ptr(), XN, YN, ZN, 1e-8, None))
+    fd = dev(torch, f)
+    torch.cuda.synchronize()
+    cb._lib.check(cb.load().ctlab_tv_gradient(fd.data_ptr(), g.data_ptr(), XN, YN, ZN, 1e-8, None))
     torch.cuda.synchronize()
     np.testing.assert_allclose(g.cpu().numpy(), ref, rtol=1e-4, atol=1e-4)
 
