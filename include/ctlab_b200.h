@@ -136,6 +136,24 @@ int ctlab_back_views(ctlab_plan *plan, const int *h_views, int n, const float *d
 int ctlab_volume_sat(ctlab_plan *plan, const float *d_vol, const unsigned char *d_mask,
                      void *stream);
 
+/* Allocation-free form of ctlab_volume_sat, for callers that cannot
+ * allocate device memory mid-reconstruction: systems that reserve their
+ * whole device-memory budget up front, or that must not let cudaMalloc /
+ * cudaFree synchronise the device behind their other streams.  Builds the
+ * FP64 volume SAT of one orientation (0: y slices -> [YN][XN+1][zp],
+ * 1: x slices -> [XN][YN+1][zp], zp >= ZN+1) of the masked volume into the
+ * caller's d_sat, with the scan's lookback scratch in a fixed 32 MiB device
+ * array inside the library (held by every GPU that loads the library until
+ * exit).  No cudaMalloc, cudaFree or allocating library call is made.
+ * Volumes whose scan needs more than 32 MiB of scratch are rejected with
+ * CTLAB_ERR_INVALID_ARG (512x512x256 needs about 23 MB).  The first call on
+ * a device looks up the array's device address; make that call before any
+ * stream capture.  All calls share the array, so calls that overlap on the
+ * GPU (other streams, other threads) race; serialise them.  Asynchronous on
+ * `stream`.  No counterpart in the reference. */
+int ctlab_volume_sat_noalloc(const float *d_vol, const unsigned char *d_mask, int XN, int YN, int ZN,
+                             int orientation, double *d_sat, int zp, void *stream);
+
 /* Copies the plan's volume SAT of one orientation to d_out (FP64 plans:
  * doubles, [planes][rows][zp] as reported by ctlab_plan_sat_layout;
  * F32PAIR plans: float pairs (hi, lo) with the same indexing). */

@@ -1,0 +1,67 @@
+"""The allocation-free volume SAT (ctlab_volume_sat_noalloc) against the plan
+path's volume SAT, through the C ABI.
+
+The entry point exists for callers that cannot allocate device memory while
+they reconstruct (a fixed, pre-reserved device-memory budget, or no implicit
+device synchronisation from cudaMalloc / cudaFree allowed): it keeps the
+scan's scratch in a fixed array inside the library.  This file is collected
+last on purpose; it passes alone in a fresh process and after the rest.
+"""
+import numpy as np
+import pytest
+
+import ctlab_b200 as cb
+from ctlab_b200 import geometry as G
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12  # FP64 SAT tolerance used by the SAT parity tests
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def test_noalloc_volume_sat_matches_plan_path_on_two_calls(torch_cuda):
+    torch = torch_cuda
+    lib = cb.load()
+    g = G.small(PN=8, XN=70, YN=45, ZN=33, start=0.0)  # views of both driving axes
+    rng = np.random.default_rng(17)
+    vol = torch.from_numpy(rng.random(g.vol_shape).astype(np.float32)).cuda()
+    mask = torch.from_numpy((rng.random(g.XN * g.YN) > 0.2).astype(np.uint8)).cuda()
+    stream = torch.cuda.current_stream().cuda_stream
+    with cb.Plan(g) as plan:
+        plan.volume_sat(vol, mask)
+        refs = {}
+        for o in (0, 1):
+            planes, rows, zp = plan.sat_layout(o)
+            buf = torch.zeros(planes * rows * zp, dtype=torch.float64, device="cuda")
+            plan.copy_volume_sat(o, buf)
+            refs[o] = (buf, planes, rows, zp)
+        torch.cuda.synchronize()
+    for call in range(2):
+        for o in (0, 1):
+            ref, planes, rows, zp = refs[o]
+            out = torch.full((planes * rows * zp,), float("nan"), dtype=torch.float64, device="cuda")
+            rc = lib.ctlab_volume_sat_noalloc(vol.data_ptr(), mask.data_ptr(), g.XN, g.YN, g.ZN, o, out.data_ptr(),
+                                              zp, stream)
+            assert rc == cb.CTLAB_OK, lib.ctlab_last_error()
+            torch.cuda.synchronize()
+            a = out.view(planes, rows, zp)[:, :, : g.ZN + 1].cpu().numpy()
+            b = ref.view(planes, rows, zp)[:, :, : g.ZN + 1].cpu().numpy()
+            assert np.all(np.isfinite(a)), f"call {call} orientation {o}: unwritten entries"
+            np.testing.assert_allclose(a, b, rtol=TOL, atol=TOL * np.abs(b).max())
+
+
+def test_noalloc_volume_sat_rejects_volumes_beyond_its_scratch(torch_cuda):
+    torch = torch_cuda
+    lib = cb.load()
+    tiny = torch.zeros(16, dtype=torch.float32, device="cuda")
+    out = torch.zeros(16, dtype=torch.float64, device="cuda")
+    rc = lib.ctlab_volume_sat_noalloc(tiny.data_ptr(), None, 2048, 2048, 1024, 0, out.data_ptr(), 1026, None)
+    assert rc == cb.CTLAB_ERR_INVALID_ARG
+    assert b"32 MiB" in lib.ctlab_last_error()
