@@ -42,7 +42,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--sat", default="fp64", choices=["fp64", "f32pair"])
+    ap.add_argument("--sat", default="fp64", choices=["fp64", "f32pair", "zprefix"])
     ap.add_argument("--cpu-views", type=int, default=4, help="views in the bounded CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -196,7 +196,7 @@ def run_ours(args):
     g = G.config2()
     hx, hy, hz = G.half_extents(g)
     ell = cb.random_ellipsoids(1 + rank, hx, hy, hz)
-    sat_mode = cb.CTLAB_SAT_FP64 if args.sat == "fp64" else cb.CTLAB_SAT_F32PAIR
+    sat_mode = {"fp64": cb.CTLAB_SAT_FP64, "f32pair": cb.CTLAB_SAT_F32PAIR, "zprefix": cb.CTLAB_SAT_ZPREFIX}[args.sat]
     plan = cb.Plan(g, device=local, sat_mode=sat_mode)
     vol = torch.zeros(g.vol_shape, dtype=torch.float32, device="cuda")
     cb.ellipsoid_phantom(vol, g, ell)

@@ -23,6 +23,7 @@ CTLAB_ERR_TIMEOUT = 5
 CTLAB_ERR_INTERNAL = 6
 CTLAB_SAT_FP64 = 0
 CTLAB_SAT_F32PAIR = 1
+CTLAB_SAT_ZPREFIX = 2
 
 _ERR_NAMES = {
     CTLAB_ERR_INVALID_ARG: "invalid argument",

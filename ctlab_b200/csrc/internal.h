@@ -119,6 +119,12 @@ cudaError_t launch_volume_sat(const float *vol, const unsigned char *mask, int X
                               int orientation, void *out, int zp, int f32pair, ScanState st,
                               int chunk, cudaStream_t s);
 
+// Column z-prefixes of the masked volume for both driving axes:
+// out[y*XN + x][k'] = sum_{z<k'} f(x, y, z), k' in [0, ZN], FP64 sums
+// rounded to FP32, column stride zpc.
+cudaError_t launch_zprefix(const float *vol, const unsigned char *mask, int XN, int YN, int ZN, float *out, int zpc,
+                           cudaStream_t s);
+
 // Projection SAT: Q[p][u'][v'] of W = prj * L (L = slab path weight of the
 // view's driving axis) for n views of the list.
 struct ProjSatArgs {
@@ -161,6 +167,8 @@ struct ProjArgs {
     int *err;             // device error word (bounded waits)
     const int *groups;    // [ngroups][G] list positions sharing a CTA (-1: empty)
     int ngroups, G;
+    const float *zprefix; // column z-prefixes [YN*XN][zp] (sat mode ZPREFIX; then zp is their stride)
+    int nbuf;             // staging depth (proj_staging)
 };
 
 // Views of one launch grouped by driving axis and angle, G per CTA.
@@ -171,7 +179,11 @@ struct ProjGroups {
 ProjGroups proj_make_groups(const HostGeometry &g, const std::vector<int> &list, int cmax);
 cudaError_t launch_proj(const ProjArgs &a, cudaStream_t s, int *launches);
 bool proj_supported(int ZN, int DNV);
-int proj_staging_columns(const HostGeometry &g, int zp);
+struct ProjStaging {
+    int cmax = 2; // staged columns per buffer
+    int nbuf = 2; // slices in flight
+};
+ProjStaging proj_staging(const HostGeometry &g, int zp, int elem_bytes);
 
 enum BackEpilogue { BACK_PLAIN = 0, BACK_SART_UPDATE = 1 };
 

@@ -35,7 +35,7 @@ void plan_free(ctlab_plan *p)
 {
     if (!p) return;
     DeviceGuard g(p->device);
-    void *bufs[] = {p->d_views, p->d_det, p->d_all_views, p->d_list, p->d_sat_y, p->d_sat_x,
+    void *bufs[] = {p->d_views, p->d_det, p->d_all_views, p->d_list, p->d_sat_y, p->d_sat_x, p->d_zprefix,
                     p->d_q, p->d_ticket, p->d_flags, p->d_agg, p->d_pref, p->d_err,
                     p->d_groups_all, p->d_groups_scratch};
     for (void *b : bufs)
@@ -48,6 +48,12 @@ void plan_free(ctlab_plan *p)
 int plan_volume_sat(ctlab_plan *p, const float *d_vol, const unsigned char *d_mask, cudaStream_t s)
 {
     const HostGeometry &g = p->g;
+    if (p->sat_mode == CTLAB_SAT_ZPREFIX) {
+        cudaError_t e = launch_zprefix(d_vol, d_mask, g.XN, g.YN, g.ZN, p->d_zprefix, p->zp, s);
+        if (e != cudaSuccess) return cuda_status(e, "column z-prefix");
+        ++p->last_launches;
+        return CTLAB_OK;
+    }
     ScanState st{p->d_ticket, p->d_flags, p->d_agg, p->d_pref, p->d_err};
     if (p->need_y) {
         cudaError_t e = launch_volume_sat(d_vol, d_mask, g.XN, g.YN, g.ZN, 0, p->d_sat_y, p->zp, p->sat_mode,
@@ -98,12 +104,14 @@ int plan_proj_list(ctlab_plan *p, const int *d_list, int n, const GroupTab &gt, 
     a.det = p->d_det;
     a.DNU = g.DNU; a.DNV = g.DNV;
     a.out = d_prj;
-    a.f32pair = p->sat_mode;
+    a.f32pair = p->sat_mode == CTLAB_SAT_F32PAIR;
+    a.zprefix = p->sat_mode == CTLAB_SAT_ZPREFIX ? p->d_zprefix : nullptr;
     a.epilogue = epilogue;
     a.meas = meas;
     a.row_sum = row_sum;
     a.resid2 = resid2;
     a.cmax = p->proj_cmax;
+    a.nbuf = p->proj_nbuf;
     a.err = p->d_err;
     a.groups = gt.d;
     a.ngroups = gt.ngroups;
@@ -127,7 +135,7 @@ int plan_proj_sat(ctlab_plan *p, const int *d_list, int n, const float *d_prj, c
     a.dx = g.dx;
     a.out = p->d_q;
     a.vp = p->vp;
-    a.f32pair = p->sat_mode;
+    a.f32pair = p->sat_mode == CTLAB_SAT_F32PAIR;
     ScanState st{p->d_ticket, p->d_flags, p->d_agg, p->d_pref, p->d_err};
     cudaError_t e = launch_proj_sat(a, st, kPrjChunk, s);
     if (e != cudaSuccess) return cuda_status(e, "projection SAT");
@@ -157,7 +165,7 @@ int plan_back_list(ctlab_plan *p, const int *d_list, int n, const unsigned char 
     a.z_lo = g.z_lo;
     a.mask = d_mask;
     a.out = d_vol;
-    a.f32pair = p->sat_mode;
+    a.f32pair = p->sat_mode == CTLAB_SAT_F32PAIR;
     a.epilogue = epilogue;
     a.col_sum = col_sum;
     a.lambda = lambda;
@@ -217,8 +225,9 @@ int ctlab_plan_create(const ctlab_geometry *geom, int device, int sat_mode, ctla
 {
     if (!geom || !out) return set_status(CTLAB_ERR_INVALID_ARG, "null geometry or output pointer");
     *out = nullptr;
-    if (sat_mode != CTLAB_SAT_FP64 && sat_mode != CTLAB_SAT_F32PAIR)
-        return set_status(CTLAB_ERR_INVALID_ARG, "sat_mode must be CTLAB_SAT_FP64 or CTLAB_SAT_F32PAIR");
+    if (sat_mode != CTLAB_SAT_FP64 && sat_mode != CTLAB_SAT_F32PAIR && sat_mode != CTLAB_SAT_ZPREFIX)
+        return set_status(CTLAB_ERR_INVALID_ARG,
+                          "sat_mode must be CTLAB_SAT_FP64, CTLAB_SAT_F32PAIR or CTLAB_SAT_ZPREFIX");
     ctlab_plan *p = new (std::nothrow) ctlab_plan();
     if (!p) return set_status(CTLAB_ERR_OOM, "host allocation failed");
     int rc = build_geometry(*geom, p->g);
@@ -244,10 +253,15 @@ int ctlab_plan_create(const ctlab_geometry *geom, int device, int sat_mode, ctla
         return set_status(CTLAB_ERR_CUDA, "cudaSetDevice failed");
     }
     for (const auto &v : g.views) (v.xdrv ? p->need_x : p->need_y) = true;
-    p->zp = round_up(g.ZN + 1, 2);
+    const bool zpre = sat_mode == CTLAB_SAT_ZPREFIX;
+    p->zp = round_up(g.ZN + 1, zpre ? 4 : 2);
     p->vp = round_up(g.DNV + 1, 2);
     p->q_capacity = g.PN;
-    p->proj_cmax = proj_staging_columns(g, p->zp);
+    {
+        const ProjStaging st = proj_staging(g, p->zp, zpre ? 4 : 8);
+        p->proj_cmax = st.cmax;
+        p->proj_nbuf = st.nbuf;
+    }
     if (g.flat_uniform) p->back_rmax = back_staging_rows(g, p->vp);
 
     long long &bytes = p->bytes;
@@ -261,8 +275,12 @@ int ctlab_plan_create(const ctlab_geometry *geom, int device, int sat_mode, ctla
     chk(dmalloc(&p->d_all_views, (size_t)g.PN, bytes));
     chk(dmalloc(&p->d_list, (size_t)g.PN, bytes));
     const size_t esz = 8; // double or float pair
-    if (p->need_y) chk(dmalloc((char **)&p->d_sat_y, esz * (size_t)g.YN * (g.XN + 1) * p->zp, bytes));
-    if (p->need_x) chk(dmalloc((char **)&p->d_sat_x, esz * (size_t)g.XN * (g.YN + 1) * p->zp, bytes));
+    if (zpre) {
+        chk(dmalloc(&p->d_zprefix, (size_t)g.XN * g.YN * p->zp, bytes));
+    } else {
+        if (p->need_y) chk(dmalloc((char **)&p->d_sat_y, esz * (size_t)g.YN * (g.XN + 1) * p->zp, bytes));
+        if (p->need_x) chk(dmalloc((char **)&p->d_sat_x, esz * (size_t)g.XN * (g.YN + 1) * p->zp, bytes));
+    }
     if (back_supported(g.DNV) && g.flat_uniform)
         chk(dmalloc((char **)&p->d_q, esz * (size_t)g.PN * (g.DNU + 1) * p->vp, bytes));
     else
@@ -274,8 +292,8 @@ int ctlab_plan_create(const ctlab_geometry *geom, int device, int sat_mode, ctla
         tiles = std::max(tiles, (size_t)planes * c);
         state = std::max(state, scan_state_doubles(planes, c, nk));
     };
-    if (p->need_y) need(g.YN, g.XN, g.ZN, kVolChunk);
-    if (p->need_x) need(g.XN, g.YN, g.ZN, kVolChunk);
+    if (p->need_y && !zpre) need(g.YN, g.XN, g.ZN, kVolChunk);
+    if (p->need_x && !zpre) need(g.XN, g.YN, g.ZN, kVolChunk);
     if (p->q_capacity) need(g.PN, g.DNU, g.DNV, kPrjChunk);
     chk(dmalloc(&p->d_ticket, 1, bytes));
     chk(dmalloc(&p->d_flags, tiles, bytes));
@@ -346,7 +364,9 @@ int ctlab_plan_sat_layout(const ctlab_plan *plan, int orientation, int *planes, 
 {
     if (!plan || !planes || !rows || !zp) return set_status(CTLAB_ERR_INVALID_ARG, "null argument");
     const HostGeometry &g = plan->g;
-    if (orientation == 0 && plan->need_y) {
+    if (plan->sat_mode == CTLAB_SAT_ZPREFIX && (orientation == 0 || orientation == 1)) {
+        *planes = g.YN; *rows = g.XN; // one array of column z-prefixes serves both axes
+    } else if (orientation == 0 && plan->need_y) {
         *planes = g.YN; *rows = g.XN + 1;
     } else if (orientation == 1 && plan->need_x) {
         *planes = g.XN; *rows = g.YN + 1;
@@ -364,8 +384,9 @@ int ctlab_copy_volume_sat(ctlab_plan *plan, int orientation, void *d_out, void *
     if (rc != CTLAB_OK) return rc;
     if (!d_out) return set_status(CTLAB_ERR_INVALID_ARG, "null output");
     DeviceGuard dg(plan->device);
-    const void *src = orientation == 0 ? plan->d_sat_y : plan->d_sat_x;
-    CTLAB_CUDA_TRY(cudaMemcpyAsync(d_out, src, 8 * (size_t)planes * rows * zp, cudaMemcpyDeviceToDevice,
+    const bool zpre = plan->sat_mode == CTLAB_SAT_ZPREFIX;
+    const void *src = zpre ? (const void *)plan->d_zprefix : (orientation == 0 ? plan->d_sat_y : plan->d_sat_x);
+    CTLAB_CUDA_TRY(cudaMemcpyAsync(d_out, src, (zpre ? 4 : 8) * (size_t)planes * rows * zp, cudaMemcpyDeviceToDevice,
                                    (cudaStream_t)stream));
     return ok();
 }

@@ -17,11 +17,13 @@ struct ctlab_plan {
     std::vector<int> h_list;
     bool need_y = false, need_x = false;
     void *d_sat_y = nullptr, *d_sat_x = nullptr;
-    int zp = 0;
+    float *d_zprefix = nullptr; // column z-prefixes (sat mode ZPREFIX)
+    int zp = 0;                 // z stride of the volume SATs / z-prefixes
     void *d_q = nullptr; // projection SATs [q_capacity][DNU+1][vp]
     int vp = 0;
     int q_capacity = 0;
     int proj_cmax = 2;  // projector staging columns
+    int proj_nbuf = 2;  // projector staging depth
     int *d_groups_all = nullptr;     // projector view groups of the full view list
     int groups_all_n = 0, groups_all_G = 1;
     int *d_groups_scratch = nullptr; // groups of a caller's view list

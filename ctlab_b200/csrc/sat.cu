@@ -336,6 +336,59 @@ cudaError_t launch_volume_sat(const float *vol, const unsigned char *mask, int X
                    : launch_scan(in, (double *)out, XN, YN, ZN, zp, st, chunk, s, kSpinLimit);
 }
 
+namespace {
+
+// One warp per voxel column: each lane sums a contiguous run of the column
+// in FP64, a warp-shuffle scan turns the lane totals into offsets, and the
+// lanes write their running sums rounded to FP32.
+__global__ void __launch_bounds__(256) zprefix_kernel(const float *__restrict__ vol, const unsigned char *mask,
+                                                      long long ncols, int ZN, float *__restrict__ out, int zpc)
+{
+    const int lane = threadIdx.x & 31;
+    const long long col = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (col >= ncols) return;
+    const float m = mask ? (mask[col] ? 1.f : 0.f) : 1.f;
+    const float *in = vol + col * ZN;
+    float *o = out + col * zpc;
+    const int per = (ZN + 31) >> 5;
+    const int k0 = lane * per;
+    double tot = 0.0;
+    for (int r = 0; r < per; ++r) {
+        const int k = k0 + r;
+        if (k < ZN) tot += (double)(__ldg(in + k) * m);
+    }
+    double incl = tot;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const double y = __shfl_up_sync(kFull, incl, d);
+        if (lane >= d) incl += y;
+    }
+    double run = __shfl_up_sync(kFull, incl, 1);
+    if (lane == 0) {
+        run = 0.0;
+        o[0] = 0.f;
+    }
+    for (int r = 0; r < per; ++r) {
+        const int k = k0 + r;
+        if (k < ZN) {
+            run += (double)(__ldg(in + k) * m);
+            o[k + 1] = (float)run;
+        }
+    }
+}
+
+} // namespace
+
+cudaError_t launch_zprefix(const float *vol, const unsigned char *mask, int XN, int YN, int ZN, float *out, int zpc,
+                           cudaStream_t s)
+{
+    const long long ncols = (long long)XN * YN;
+    const long long blocks = (ncols * 32 + 255) / 256;
+    if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    zprefix_kernel<<<(unsigned)blocks, 256, 0, s>>>(vol, mask, ncols, ZN, out, zpc);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_scan_stall(const float *vol, int rows, int nk, void *out, ScanState st, int chunk,
                               unsigned spin_limit, cudaStream_t s)
 {

@@ -61,7 +61,7 @@ def make_case(name):
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
-@pytest.mark.parametrize("sat_mode", [cb.CTLAB_SAT_FP64, cb.CTLAB_SAT_F32PAIR])
+@pytest.mark.parametrize("sat_mode", [cb.CTLAB_SAT_FP64, cb.CTLAB_SAT_F32PAIR, cb.CTLAB_SAT_ZPREFIX])
 def test_projection_matches_oracle(torch_cuda, name, sat_mode):
     torch = torch_cuda
     g = make_case(name)
@@ -121,6 +121,18 @@ def test_volume_sat_matches_oracle(torch_cuda):
                 s = s[:, :, : g.ZN + 1]
                 assert s.shape == ref.shape
                 np.testing.assert_allclose(s, ref, rtol=tol, atol=tol * np.abs(ref).max())
+    # column z-prefixes (ZPREFIX plans): FP64 sums rounded to FP32
+    masked = vol.astype(np.float64) * mask.reshape(g.YN, g.XN, 1)
+    zref = np.concatenate([np.zeros((g.YN, g.XN, 1)), np.cumsum(masked, axis=2)], axis=2)
+    with cb.Plan(g, sat_mode=cb.CTLAB_SAT_ZPREFIX) as plan:
+        plan.volume_sat(dev(torch, vol), dev(torch, mask))
+        planes, rows, zp = plan.sat_layout(0)
+        assert (planes, rows) == (g.YN, g.XN) and zp >= g.ZN + 1
+        buf = torch.zeros(planes * rows * zp, dtype=torch.float32, device="cuda")
+        plan.copy_volume_sat(0, buf)
+        torch.cuda.synchronize()
+        zs = buf.cpu().numpy().reshape(planes, rows, zp)[:, :, : g.ZN + 1]
+        np.testing.assert_allclose(zs, zref, rtol=1e-6, atol=1e-7 * np.abs(zref).max())
 
 
 def test_config1_views_match_oracle(torch_cuda):
@@ -147,7 +159,8 @@ def test_config1_views_match_oracle(torch_cuda):
         assert rel_l2(vb.cpu().numpy(), ref_b) <= REL_L2
 
 
-def test_config2_views_match_oracle(torch_cuda):
+@pytest.mark.parametrize("sat_mode", [cb.CTLAB_SAT_FP64, cb.CTLAB_SAT_ZPREFIX])
+def test_config2_views_match_oracle(torch_cuda, sat_mode):
     torch = torch_cuda
     g = G.config2()
     hx, hy, hz = G.half_extents(g)
@@ -159,18 +172,18 @@ def test_config2_views_match_oracle(torch_cuda):
     gs = g.with_views(views)
     vol_h = vol.cpu().numpy()
     ref_p = oracle.dd3_proj(gs, vol_h)
-    with cb.Plan(g) as plan:
+    with cb.Plan(g, sat_mode=sat_mode) as plan:
         out = torch.zeros((len(views), g.DNU, g.DNV), dtype=torch.float32, device="cuda")
         plan.proj_views(views, vol, out)
         torch.cuda.synchronize()
         got = out.cpu().numpy()
-        record_error("proj/config2_4views", rel_l2(got, ref_p))
+        record_error(f"proj/config2_4views/sat{sat_mode}", rel_l2(got, ref_p))
         assert rel_l2(got, ref_p) <= REL_L2
         ref_b = oracle.dd3_back(gs, got)
         vb = torch.zeros(g.vol_shape, dtype=torch.float32, device="cuda")
         plan.back_views(views, out, vb)
         torch.cuda.synchronize()
-        record_error("back/config2_4views", rel_l2(vb.cpu().numpy(), ref_b))
+        record_error(f"back/config2_4views/sat{sat_mode}", rel_l2(vb.cpu().numpy(), ref_b))
         assert rel_l2(vb.cpu().numpy(), ref_b) <= REL_L2
 
 
