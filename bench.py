@@ -46,7 +46,17 @@ def parse():
     ap.add_argument("--cpu-views", type=int, default=4, help="views in the bounded CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--views", type=int, default=0,
+                    help="profiling case: keep only this many evenly spaced views of the 984 (0 = all)")
     return ap.parse_args()
+
+
+def workload_geometry(args):
+    from ctlab_b200 import geometry as G
+    g = G.config2()
+    if args.views:
+        g = g.with_views(np.linspace(0, g.PN - 1, args.views).round().astype(int))
+    return g
 
 
 def dist_env():
@@ -65,7 +75,8 @@ def peaks():
 
 
 def config_dict(args, extra=None):
-    d = {"workload": WORKLOAD, "volume": [512, 512, 256], "views": 984, "detector": [888, 64],
+    d = {"workload": WORKLOAD if not args.views else f"{WORKLOAD}_subset{args.views}v",
+         "volume": [512, 512, 256], "views": args.views or 984, "detector": [888, 64],
          "voxel_mm": [1.0, 1.0, 0.15625], "cell_mm": [1.0239, 1.0960], "sod_sdd_mm": [541, 949],
          "sat": args.sat, "l2": "inputs larger than L2 (volume 268 MB, SATs 1.08 GB)",
          "phantom": "random ellipsoids, 20-40, seed 1+rank"}
@@ -193,7 +204,7 @@ def run_ours(args):
         dist.init_process_group("nccl", init_method="env://", world_size=ws, rank=rank,
                                 timeout=__import__("datetime").timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
-    g = G.config2()
+    g = workload_geometry(args)
     hx, hy, hz = G.half_extents(g)
     ell = cb.random_ellipsoids(1 + rank, hx, hy, hz)
     sat_mode = {"fp64": cb.CTLAB_SAT_FP64, "f32pair": cb.CTLAB_SAT_F32PAIR, "zprefix": cb.CTLAB_SAT_ZPREFIX}[args.sat]
@@ -259,7 +270,7 @@ def run_ours(args):
     t_proj, t_back = float(np.mean(proj_k)), float(np.mean(back_k))
     peak, peak_kind = peaks()
     alg = 8.0 * vv + 4.0 * g.PN * g.DNU * g.DNV  # bytes per launch (proj or back)
-    dom = "dd3_proj_kernel" if t_proj >= t_back else "dd3_back_kernel"
+    dom = ("dd3_proj_zp_kernel" if args.sat == "zprefix" else "dd3_proj_kernel") if t_proj >= t_back else "dd3_back_kernel"
     t_dom = max(t_proj, t_back)
     achieved = alg / (t_dom * 1e-3) / 1e9
     traffic = None
@@ -307,7 +318,8 @@ def run_ours(args):
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32 (f64 SAT)" if args.sat == "fp64" else "f32 (f32-pair SAT)",
+            "vs_baseline": None, "dtype": {"fp64": "f32 (f64 SAT)", "f32pair": "f32 (f32-pair SAT)",
+                                            "zprefix": "f32 (f64-accumulated z-prefix SAT)"}[args.sat],
             "data": "synthetic (seeded random-ellipsoid phantoms)",
             "config": config_dict(args, {"parallelism": f"independent volume per GPU x{ws}"}),
             "clocks": clk.summary(),
