@@ -1,5 +1,6 @@
 // Host-side geometry: validation, detector boundaries and per-view constants,
 // all in FP64.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdarg>
@@ -169,6 +170,43 @@ std::vector<double> det_table_host(const HostGeometry &g)
     std::copy(g.bz.begin(), g.bz.end(), h.begin() + t.off_bz);
     std::copy(g.vz.begin(), g.vz.end(), h.begin() + t.off_vz);
     return h;
+}
+
+std::vector<std::vector<int>> view_runs(const HostGeometry &g, const std::vector<int> &list)
+{
+    std::vector<std::vector<int>> runs;
+    for (int axis = 0; axis < 2; ++axis) {
+        std::vector<std::pair<double, int>> ang;
+        for (int pos = 0; pos < (int)list.size(); ++pos) {
+            const DevView &V = g.views[list[pos]];
+            if (V.xdrv != axis) continue;
+            double th = std::atan2(V.s, V.c);
+            if (th < 0) th += kTwoPi;
+            ang.push_back({th, pos});
+        }
+        if (ang.empty()) continue;
+        std::stable_sort(ang.begin(), ang.end(),
+                         [](const std::pair<double, int> &a, const std::pair<double, int> &b) { return a.first < b.first; });
+        // a gap wider than 4x the median spacing starts a new run
+        std::vector<double> gaps;
+        for (size_t i = 1; i < ang.size(); ++i) gaps.push_back(ang[i].first - ang[i - 1].first);
+        double med = 0.0;
+        if (!gaps.empty()) {
+            std::vector<double> s2 = gaps;
+            std::nth_element(s2.begin(), s2.begin() + s2.size() / 2, s2.end());
+            med = s2[s2.size() / 2];
+        }
+        std::vector<int> cur{ang[0].second};
+        for (size_t i = 1; i < ang.size(); ++i) {
+            if (gaps[i - 1] > 4.0 * med + 1e-12) {
+                runs.push_back(cur);
+                cur.clear();
+            }
+            cur.push_back(ang[i].second);
+        }
+        runs.push_back(cur);
+    }
+    return runs;
 }
 
 } // namespace ctlab

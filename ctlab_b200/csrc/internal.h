@@ -1,6 +1,7 @@
 // Internal declarations shared by the libctlab_b200 translation units.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -95,6 +96,10 @@ __host__ __device__ inline DetTable det_table_layout(int DNU, int DNV)
 }
 std::vector<double> det_table_host(const HostGeometry &g);
 
+// Positions of `list` (view indices) split by driving axis into runs of
+// angularly adjacent views, each run sorted by angle.
+std::vector<std::vector<int>> view_runs(const HostGeometry &g, const std::vector<int> &list);
+
 // ----------------------------------------------------------------------
 // kernels (launchers return cudaError_t from the launch)
 // ----------------------------------------------------------------------
@@ -119,11 +124,12 @@ cudaError_t launch_volume_sat(const float *vol, const unsigned char *mask, int X
                               int orientation, void *out, int zp, int f32pair, ScanState st,
                               int chunk, cudaStream_t s);
 
-// Column z-prefixes of the masked volume for both driving axes:
-// out[y*XN + x][k'] = sum_{z<k'} f(x, y, z), k' in [0, ZN], FP64 sums
-// rounded to FP32, column stride zpc.
-cudaError_t launch_zprefix(const float *vol, const unsigned char *mask, int XN, int YN, int ZN, float *out, int zpc,
-                           cudaStream_t s);
+// Slice-major column z-prefixes of the masked volume for one driving axis:
+// out[j][k][c] = sum_{z<k} f(column c of slice j, z), k in [0, ZN], FP64
+// sums rounded to FP32, row stride rs >= nb (pad columns zero).
+// orientation 0: slices y, columns x (Z_y); 1: slices x, columns y (Z_x).
+cudaError_t launch_zt(const float *vol, const unsigned char *mask, int XN, int YN, int ZN, int orientation,
+                      float *out, int rs, cudaStream_t s);
 
 // Projection SAT: Q[p][u'][v'] of W = prj * L (L = slab path weight of the
 // view's driving axis) for n views of the list.
@@ -167,8 +173,12 @@ struct ProjArgs {
     int *err;             // device error word (bounded waits)
     const int *groups;    // [ngroups][G] list positions sharing a CTA (-1: empty)
     int ngroups, G;
-    const float *zprefix; // column z-prefixes [YN*XN][zp] (sat mode ZPREFIX; then zp is their stride)
     int nbuf;             // staging depth (proj_staging)
+    // slice-major z-prefix projector (sat mode ZPREFIX)
+    const float *zt_y, *zt_x; // [YN][ZN+1][zt_rs_y], [XN][ZN+1][zt_rs_x]
+    int zt_rs_y, zt_rs_x;
+    int t_cb, t_kb, t_kr;     // stage: [t_kr][t_cb] floats, TMA boxes of t_kb rows
+    int t_nstage, t_nw, t_ep, t_gtab;
 };
 
 // Views of one launch grouped by driving axis and angle, G per CTA.
@@ -184,6 +194,20 @@ struct ProjStaging {
     int nbuf = 2; // slices in flight
 };
 ProjStaging proj_staging(const HostGeometry &g, int zp, int elem_bytes);
+
+// Staging of the slice-major z-prefix projector: G views per CTA, NR
+// detector rows per consumer warp (NW warps), stages of KR rows x CB
+// columns (TMA boxes of KB rows), nstage stages, EP floats per view of
+// detector z boundaries.
+struct ProjTStaging {
+    int G = 1, NR = 1, NW = 1, CB = 0, KB = 0, KR = 0, nstage = 2, EP = 4;
+    size_t smem = 0;
+    bool ok = false;
+};
+ProjTStaging proj_t_staging(const HostGeometry &g);
+ProjGroups proj_t_make_groups(const HostGeometry &g, const std::vector<int> &list, const ProjTStaging &st);
+cudaError_t launch_proj_t(const ProjArgs &a, const ProjTStaging &st, const CUtensorMap &tmy, const CUtensorMap &tmx,
+                          cudaStream_t s, int *launches);
 
 enum BackEpilogue { BACK_PLAIN = 0, BACK_SART_UPDATE = 1 };
 

@@ -1,5 +1,7 @@
 // Plans and the device-pointer C ABI: geometry upload, SAT workspaces,
 // stream-ordered projection / backprojection.
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -29,13 +31,46 @@ cudaError_t dmalloc(T **p, size_t n, long long &bytes)
     return e;
 }
 
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime
+// (no link-time dependency on libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// TMA map of a slice-major z-prefix array [na][ZN+1][rs] (nb valid columns):
+// boxes of CB columns x KB rows x 1 slice, zero fill outside.
+int encode_zt_map(CUtensorMap *m, float *base, int nb, int ZN, int na, int rs, int CB, int KB)
+{
+    PFN_cuTensorMapEncodeTiled_v12000 fn = tensor_map_encoder();
+    if (!fn) return set_status(CTLAB_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    const cuuint64_t dims[3] = {(cuuint64_t)nb, (cuuint64_t)ZN + 1, (cuuint64_t)na};
+    const cuuint64_t strides[2] = {(cuuint64_t)rs * 4, (cuuint64_t)(ZN + 1) * rs * 4};
+    const cuuint32_t box[3] = {(cuuint32_t)CB, (cuuint32_t)KB, 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, es,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_status(CTLAB_ERR_CUDA, "cuTensorMapEncodeTiled failed for a z-prefix array");
+    return CTLAB_OK;
+}
+
 } // namespace
 
 void plan_free(ctlab_plan *p)
 {
     if (!p) return;
     DeviceGuard g(p->device);
-    void *bufs[] = {p->d_views, p->d_det, p->d_all_views, p->d_list, p->d_sat_y, p->d_sat_x, p->d_zprefix,
+    void *bufs[] = {p->d_views, p->d_det, p->d_all_views, p->d_list, p->d_sat_y, p->d_sat_x, p->d_zt_y, p->d_zt_x,
                     p->d_q, p->d_ticket, p->d_flags, p->d_agg, p->d_pref, p->d_err,
                     p->d_groups_all, p->d_groups_scratch};
     for (void *b : bufs)
@@ -49,9 +84,16 @@ int plan_volume_sat(ctlab_plan *p, const float *d_vol, const unsigned char *d_ma
 {
     const HostGeometry &g = p->g;
     if (p->sat_mode == CTLAB_SAT_ZPREFIX) {
-        cudaError_t e = launch_zprefix(d_vol, d_mask, g.XN, g.YN, g.ZN, p->d_zprefix, p->zp, s);
-        if (e != cudaSuccess) return cuda_status(e, "column z-prefix");
-        ++p->last_launches;
+        if (p->need_y) {
+            cudaError_t e = launch_zt(d_vol, d_mask, g.XN, g.YN, g.ZN, 0, p->d_zt_y, p->zt_rs_y, s);
+            if (e != cudaSuccess) return cuda_status(e, "z-prefixes (y slices)");
+            ++p->last_launches;
+        }
+        if (p->need_x) {
+            cudaError_t e = launch_zt(d_vol, d_mask, g.XN, g.YN, g.ZN, 1, p->d_zt_x, p->zt_rs_x, s);
+            if (e != cudaSuccess) return cuda_status(e, "z-prefixes (x slices)");
+            ++p->last_launches;
+        }
         return CTLAB_OK;
     }
     ScanState st{p->d_ticket, p->d_flags, p->d_agg, p->d_pref, p->d_err};
@@ -75,7 +117,8 @@ int plan_groups(ctlab_plan *p, const std::vector<int> &host_list, int *d_dst, in
 {
     std::vector<int> ids(host_list.size());
     for (size_t i = 0; i < host_list.size(); ++i) ids[i] = host_list[i];
-    ProjGroups pg = proj_make_groups(p->g, ids, p->proj_cmax);
+    ProjGroups pg = p->sat_mode == CTLAB_SAT_ZPREFIX ? proj_t_make_groups(p->g, ids, p->tst)
+                                                     : proj_make_groups(p->g, ids, p->proj_cmax);
     if ((int)pg.table.size() > cap) return set_status(CTLAB_ERR_INTERNAL, "group table capacity exceeded");
     if (!pg.table.empty()) {
         CTLAB_CUDA_TRY(cudaMemcpyAsync(d_dst, pg.table.data(), sizeof(int) * pg.table.size(), cudaMemcpyHostToDevice, s));
@@ -105,7 +148,6 @@ int plan_proj_list(ctlab_plan *p, const int *d_list, int n, const GroupTab &gt, 
     a.DNU = g.DNU; a.DNV = g.DNV;
     a.out = d_prj;
     a.f32pair = p->sat_mode == CTLAB_SAT_F32PAIR;
-    a.zprefix = p->sat_mode == CTLAB_SAT_ZPREFIX ? p->d_zprefix : nullptr;
     a.epilogue = epilogue;
     a.meas = meas;
     a.row_sum = row_sum;
@@ -116,6 +158,23 @@ int plan_proj_list(ctlab_plan *p, const int *d_list, int n, const GroupTab &gt, 
     a.groups = gt.d;
     a.ngroups = gt.ngroups;
     a.G = gt.G;
+    if (p->sat_mode == CTLAB_SAT_ZPREFIX) {
+        const ProjTStaging &st = p->tst;
+        a.zt_y = p->d_zt_y;
+        a.zt_x = p->d_zt_x;
+        a.zt_rs_y = p->zt_rs_y;
+        a.zt_rs_x = p->zt_rs_x;
+        a.t_cb = st.CB;
+        a.t_kb = st.KB;
+        a.t_kr = st.KR;
+        a.t_nstage = st.nstage;
+        a.t_nw = st.NW;
+        a.t_ep = st.EP;
+        a.t_gtab = st.G;
+        cudaError_t e = launch_proj_t(a, st, p->tm_y, p->tm_x, s, &p->last_launches);
+        if (e != cudaSuccess) return cuda_status(e, "DD3 projection kernel (z-prefix)");
+        return CTLAB_OK;
+    }
     cudaError_t e = launch_proj(a, s, &p->last_launches);
     if (e != cudaSuccess) return cuda_status(e, "DD3 projection kernel");
     return CTLAB_OK;
@@ -254,11 +313,19 @@ int ctlab_plan_create(const ctlab_geometry *geom, int device, int sat_mode, ctla
     }
     for (const auto &v : g.views) (v.xdrv ? p->need_x : p->need_y) = true;
     const bool zpre = sat_mode == CTLAB_SAT_ZPREFIX;
-    p->zp = round_up(g.ZN + 1, zpre ? 4 : 2);
+    p->zp = round_up(g.ZN + 1, 2);
     p->vp = round_up(g.DNV + 1, 2);
     p->q_capacity = g.PN;
-    {
-        const ProjStaging st = proj_staging(g, p->zp, zpre ? 4 : 8);
+    if (zpre) {
+        p->tst = proj_t_staging(g);
+        if (!p->tst.ok) {
+            delete p;
+            return set_status(CTLAB_ERR_UNSUPPORTED, "DNV beyond the z-prefix projector's tiles");
+        }
+        p->zt_rs_y = round_up(g.XN, 4);
+        p->zt_rs_x = round_up(g.YN, 4);
+    } else {
+        const ProjStaging st = proj_staging(g, p->zp, 8);
         p->proj_cmax = st.cmax;
         p->proj_nbuf = st.nbuf;
     }
@@ -276,7 +343,8 @@ int ctlab_plan_create(const ctlab_geometry *geom, int device, int sat_mode, ctla
     chk(dmalloc(&p->d_list, (size_t)g.PN, bytes));
     const size_t esz = 8; // double or float pair
     if (zpre) {
-        chk(dmalloc(&p->d_zprefix, (size_t)g.XN * g.YN * p->zp, bytes));
+        if (p->need_y) chk(dmalloc(&p->d_zt_y, (size_t)g.YN * (g.ZN + 1) * p->zt_rs_y, bytes));
+        if (p->need_x) chk(dmalloc(&p->d_zt_x, (size_t)g.XN * (g.ZN + 1) * p->zt_rs_x, bytes));
     } else {
         if (p->need_y) chk(dmalloc((char **)&p->d_sat_y, esz * (size_t)g.YN * (g.XN + 1) * p->zp, bytes));
         if (p->need_x) chk(dmalloc((char **)&p->d_sat_x, esz * (size_t)g.XN * (g.YN + 1) * p->zp, bytes));
@@ -306,6 +374,16 @@ int ctlab_plan_create(const ctlab_geometry *geom, int device, int sat_mode, ctla
     if (e != cudaSuccess) {
         plan_free(p);
         return cuda_status(e, "plan workspace allocation");
+    }
+    if (zpre && p->tst.CB > 0) {
+        int rc2 = CTLAB_OK;
+        if (p->need_y) rc2 = encode_zt_map(&p->tm_y, p->d_zt_y, g.XN, g.ZN, g.YN, p->zt_rs_y, p->tst.CB, p->tst.KB);
+        if (rc2 == CTLAB_OK && p->need_x)
+            rc2 = encode_zt_map(&p->tm_x, p->d_zt_x, g.YN, g.ZN, g.XN, p->zt_rs_x, p->tst.CB, p->tst.KB);
+        if (rc2 != CTLAB_OK) {
+            plan_free(p);
+            return rc2;
+        }
     }
     std::vector<int> all(g.PN);
     for (int i = 0; i < g.PN; ++i) all[i] = i;
@@ -364,8 +442,15 @@ int ctlab_plan_sat_layout(const ctlab_plan *plan, int orientation, int *planes, 
 {
     if (!plan || !planes || !rows || !zp) return set_status(CTLAB_ERR_INVALID_ARG, "null argument");
     const HostGeometry &g = plan->g;
-    if (plan->sat_mode == CTLAB_SAT_ZPREFIX && (orientation == 0 || orientation == 1)) {
-        *planes = g.YN; *rows = g.XN; // one array of column z-prefixes serves both axes
+    if (plan->sat_mode == CTLAB_SAT_ZPREFIX) {
+        if (orientation == 0 && plan->need_y) {
+            *planes = g.YN; *rows = g.ZN + 1; *zp = plan->zt_rs_y;
+        } else if (orientation == 1 && plan->need_x) {
+            *planes = g.XN; *rows = g.ZN + 1; *zp = plan->zt_rs_x;
+        } else {
+            return set_status(CTLAB_ERR_INVALID_ARG, "orientation not used by this plan's views");
+        }
+        return ok();
     } else if (orientation == 0 && plan->need_y) {
         *planes = g.YN; *rows = g.XN + 1;
     } else if (orientation == 1 && plan->need_x) {
@@ -385,7 +470,8 @@ int ctlab_copy_volume_sat(ctlab_plan *plan, int orientation, void *d_out, void *
     if (!d_out) return set_status(CTLAB_ERR_INVALID_ARG, "null output");
     DeviceGuard dg(plan->device);
     const bool zpre = plan->sat_mode == CTLAB_SAT_ZPREFIX;
-    const void *src = zpre ? (const void *)plan->d_zprefix : (orientation == 0 ? plan->d_sat_y : plan->d_sat_x);
+    const void *src = zpre ? (const void *)(orientation == 0 ? plan->d_zt_y : plan->d_zt_x)
+                           : (orientation == 0 ? plan->d_sat_y : plan->d_sat_x);
     CTLAB_CUDA_TRY(cudaMemcpyAsync(d_out, src, (zpre ? 4 : 8) * (size_t)planes * rows * zp, cudaMemcpyDeviceToDevice,
                                    (cudaStream_t)stream));
     return ok();

@@ -17,8 +17,11 @@ struct ctlab_plan {
     std::vector<int> h_list;
     bool need_y = false, need_x = false;
     void *d_sat_y = nullptr, *d_sat_x = nullptr;
-    float *d_zprefix = nullptr; // column z-prefixes (sat mode ZPREFIX)
-    int zp = 0;                 // z stride of the volume SATs / z-prefixes
+    float *d_zt_y = nullptr, *d_zt_x = nullptr; // slice-major z-prefixes (sat mode ZPREFIX)
+    int zt_rs_y = 0, zt_rs_x = 0;               // their row strides (floats)
+    CUtensorMap tm_y, tm_x;                     // TMA maps of the z-prefix arrays
+    ctlab::ProjTStaging tst;                    // z-prefix projector staging
+    int zp = 0;                 // z stride of the volume SATs
     void *d_q = nullptr; // projection SATs [q_capacity][DNU+1][vp]
     int vp = 0;
     int q_capacity = 0;

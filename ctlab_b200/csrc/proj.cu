@@ -143,60 +143,6 @@ __device__ __forceinline__ void phase_a(const SliceInfo &in, const int2 *cf, flo
     }
 }
 
-// Phase A on staged column z-prefixes (sat mode CTLAB_SAT_ZPREFIX): column c
-// holds C_c(k) = sum_{z<k} f(c, z) in FP32 (accumulated in FP64), so
-//   D = (S_c' - S_c) + f' C_c' - f C_c,  S_c' - S_c = sum_{c <= i < c'} C_i,
-// the same FP32 quantities the 2-D SAT path forms after its FP64 column
-// differences, with one load per boundary and row.
-template <int QPER>
-__device__ __forceinline__ void phase_a_zp(const SliceInfo &in, const int2 *cf, float *D, int ds, const float *S,
-                                           int kstr, const float *Sg, long long scol, int tid)
-{
-    constexpr int kGroups = kU / QPER;
-    constexpr int mstep = kThreads / kGroups;
-    const int ks = max(in.k_lo, 1);
-    const int half = (in.k_hi - ks + 2) >> 1;
-    const int g = tid / mstep, m0 = tid - g * mstep;
-    const int qa = g * QPER;
-    int cq[QPER + 1];
-    float fq[QPER + 1];
-#pragma unroll
-    for (int i = 0; i <= QPER; ++i) {
-        const int2 e = cf[qa + i];
-        cq[i] = e.x;
-        fq[i] = __int_as_float(e.y);
-    }
-    for (int m = m0; m < half; m += mstep) {
-        const int k = ks + m;
-        const int k1 = min(k + half, in.k_hi); // odd count: the last row repeats
-#pragma unroll 1
-        for (int h = 0; h < 2; ++h) {
-            const int kk = h ? k1 : k;
-            auto col = [&](int c) -> float {
-                return in.fits ? S[c * kstr + (kk - in.k_lo_a)] : Sg[(long long)c * scol + kk];
-            };
-            float cv[QPER + 1];
-#pragma unroll
-            for (int i = 0; i <= QPER; ++i) cv[i] = col(cq[i]);
-#pragma unroll
-            for (int i = 1; i <= QPER; ++i) {
-                const int dc = cq[i] - cq[i - 1];
-                float dS = 0.f;
-                if (dc == 1) {
-                    dS = cv[i - 1];
-                } else if (dc == -1) {
-                    dS = -cv[i];
-                } else if (dc != 0) { // cells wider than a column
-                    const int lo = min(cq[i], cq[i - 1]), hi = max(cq[i], cq[i - 1]);
-                    for (int c = lo; c < hi; ++c) dS += col(c);
-                    if (dc < 0) dS = -dS;
-                }
-                D[(qa + i - 1) * ds + kk] = dS + (fq[i] * cv[i] - fq[i - 1] * cv[i - 1]);
-            }
-        }
-    }
-}
-
 template <int NR, int G, class T>
 __global__ void __launch_bounds__(kThreads, 1) dd3_proj_kernel(ProjArgs a, int ds, int cmax, int kstr)
 {
@@ -226,15 +172,13 @@ __global__ void __launch_bounds__(kThreads, 1) dd3_proj_kernel(ProjArgs a, int d
     __syncthreads();
     const DevView &V0 = a.views[a.view_list[s_pos_list[0]]]; // all views share the axis
     const int na = V0.na, nb = V0.nb;
-    // column (slice j, in-plane index c) starts at sat + j*s_slice + c*s_col:
-    // 2-D SATs hold nb+1 boundary columns per slice; column z-prefixes
-    // (one array for both axes) hold the nb voxel columns
-    constexpr bool ZP = std::is_same<T, float>::value;
+    // column (slice j, boundary column c) starts at sat + j*s_slice + c*s_col:
+    // 2-D SATs hold nb+1 boundary columns per slice
     constexpr int kAlign = 16 / (int)sizeof(T); // elements per 16 bytes
-    const T *sat = reinterpret_cast<const T *>(ZP ? a.zprefix : (V0.xdrv ? a.sat_x : a.sat_y));
-    const long long s_col = ZP ? (V0.xdrv ? (long long)a.XN * zp : (long long)zp) : (long long)zp;
-    const long long s_slice = ZP ? (V0.xdrv ? (long long)zp : (long long)a.XN * zp) : (long long)(nb + 1) * zp;
-    const int ccap = ZP ? nb - 1 : nb; // last column index
+    const T *sat = reinterpret_cast<const T *>(V0.xdrv ? a.sat_x : a.sat_y);
+    const long long s_col = zp;
+    const long long s_slice = (long long)(nb + 1) * zp;
+    const int ccap = nb; // last column index
     auto view_of = [&](int g) -> const DevView & {
         const int ps = s_pos_list[g] >= 0 ? s_pos_list[g] : s_pos_list[0];
         return a.views[a.view_list[ps]];
@@ -290,7 +234,7 @@ __global__ void __launch_bounds__(kThreads, 1) dd3_proj_kernel(ProjArgs a, int d
         // one column of margin each side: interior boundaries may round past
         // the end boundaries' range by an ulp
         i_lo = max((int)xmin - 1, 0);
-        ncols = min((int)xmax + (ZP ? 1 : 2), ccap) - i_lo + 1;
+        ncols = min((int)xmax + 2, ccap) - i_lo + 1;
     };
     // boundary positions of slice j into slot j % (nbuf+1) (threads 0 .. G*(kU+1)-1)
     auto set_pos = [&](int j) {
@@ -302,7 +246,7 @@ __global__ void __launch_bounds__(kThreads, 1) dd3_proj_kernel(ProjArgs a, int d
             const int i = min((int)xc, nb - 1);
             int i_lo, ncols;
             col_range(j, i_lo, ncols);
-            const int c = (ncols <= cmax) ? min(max(i - i_lo, 0), ncols - (ZP ? 1 : 2)) : i;
+            const int c = (ncols <= cmax) ? min(max(i - i_lo, 0), ncols - 2) : i;
             s_pos[sl][g][q] = x;
             s_cf[sl][g][q] = make_int2(c, __float_as_int((float)(xc - (double)i)));
         }
@@ -393,15 +337,9 @@ __global__ void __launch_bounds__(kThreads, 1) dd3_proj_kernel(ProjArgs a, int d
             if (!timed_out) {
                 // pick the boundaries per thread so that one pass of the
                 // thread rows covers the SAT rows (mstep = kThreads*QPER/kU)
-                if constexpr (ZP) {
-                    if (half > kThreads / 8) phase_a_zp<8>(in, s_cf[js][g], D, ds, S, kstr, Sg, s_col, tid);
-                    else if (half > kThreads / 16) phase_a_zp<4>(in, s_cf[js][g], D, ds, S, kstr, Sg, s_col, tid);
-                    else phase_a_zp<2>(in, s_cf[js][g], D, ds, S, kstr, Sg, s_col, tid);
-                } else {
-                    if (half > kThreads / 8) phase_a<8, T>(in, s_cf[js][g], D, ds, S, kstr, Sg, s_col, tid);
-                    else if (half > kThreads / 16) phase_a<4, T>(in, s_cf[js][g], D, ds, S, kstr, Sg, s_col, tid);
-                    else phase_a<2, T>(in, s_cf[js][g], D, ds, S, kstr, Sg, s_col, tid);
-                }
+                if (half > kThreads / 8) phase_a<8, T>(in, s_cf[js][g], D, ds, S, kstr, Sg, s_col, tid);
+                else if (half > kThreads / 16) phase_a<4, T>(in, s_cf[js][g], D, ds, S, kstr, Sg, s_col, tid);
+                else phase_a<2, T>(in, s_cf[js][g], D, ds, S, kstr, Sg, s_col, tid);
             }
             __syncthreads();
             if (g == G - 1 || s_pos_list[g + 1] < 0) {
@@ -477,359 +415,6 @@ __global__ void __launch_bounds__(kThreads, 1) dd3_proj_kernel(ProjArgs a, int d
     }
 }
 
-// Projector on staged column z-prefixes (sat mode CTLAB_SAT_ZPREFIX).
-//
-// Warp-specialised: one producer warp walks the slices ahead of the others,
-// computes each slice's staged column range, z range and the boundary
-// columns/fractions of every view, and issues the bulk copies of the staged
-// column z-prefixes into a ring of nbuf buffers.  Per buffer a "full"
-// mbarrier (32 producer arrivals + the copies' bytes) hands a slice to the
-// consumers and an "empty" mbarrier (one arrival per consumer warp) hands the
-// buffer back, so no CTA-wide barrier sits in the slice loop.
-//
-// No strip array: every consumer thread owns one detector column u of the
-// tile and NR consecutive detector rows, and for each of its NR+1 z
-// boundaries w evaluates the strip integral between the column's two
-// boundary rays directly at the two SAT rows around kz = Z0 + T_u(j) e_w:
-//   D_u(k) = (S_cb - S_ca)(k) + f_b C_cb(k) - f_a C_ca(k),
-// C_c(k) the staged FP32 z-prefix of column c (FP64 sums, rounded once), and
-// S_cb - S_ca the sum of C over the columns between (0 or one column for
-// cells narrower than a voxel).  Lanes 0-15 / 16-31 of a warp hold two
-// adjacent columns and 16 row segments each.
-constexpr int kConsumerWarps = kThreads / 32;
-constexpr int kZpThreads = kThreads + 32;
-
-template <int NR, int G>
-__global__ void __launch_bounds__(kZpThreads, 1) dd3_proj_zp_kernel(ProjArgs a, int cmax, int kstr)
-{
-    extern __shared__ __align__(128) unsigned char smem[];
-    const int nbuf = a.nbuf;
-    float *colbuf = reinterpret_cast<float *>(smem);             // [nbuf][cmax][kstr]
-    float *s_e = colbuf + (size_t)nbuf * cmax * kstr;            // [G][DNV+1]
-    __shared__ __align__(8) uint64_t s_full[kMaxBuf], s_empty[kMaxBuf];
-    __shared__ SliceInfo s_info[kMaxBuf];
-    __shared__ double s_c0[G][kU + 1], s_m[G][kU + 1];
-    __shared__ double s_r[G][kU];
-    __shared__ int2 s_cf[kMaxBuf][G][kU + 1]; // per view and boundary: staged column, fraction bits
-    __shared__ int s_pos_list[G];
-    __shared__ double s_ga0[G];
-    __shared__ float s_Z0[G];
-    __shared__ int s_abort;
-
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid < G) s_pos_list[tid] = a.groups[blockIdx.y * G + tid];
-    if (tid == 0) s_abort = 0;
-    const int u0 = blockIdx.x * kU;
-    const int nu = min(kU, a.DNU - u0);
-    const DetTable t = det_table_layout(a.DNU, a.DNV);
-    const double *det = a.det;
-    const int ZN = a.ZN, DNV = a.DNV, zp = a.zp;
-    const double dx = a.dx;
-    __syncthreads();
-    const DevView &V0 = a.views[a.view_list[s_pos_list[0]]];
-    const int na = V0.na, nb = V0.nb;
-    const float *sat = a.zprefix;
-    const long long s_col = V0.xdrv ? (long long)a.XN * zp : (long long)zp;
-    const long long s_slice = V0.xdrv ? (long long)zp : (long long)a.XN * zp;
-    auto view_of = [&](int g) -> const DevView & {
-        const int ps = s_pos_list[g] >= 0 ? s_pos_list[g] : s_pos_list[0];
-        return a.views[a.view_list[ps]];
-    };
-
-    if (tid == 0) {
-        for (int i = 0; i < nbuf; ++i) {
-            mbar_init(&s_full[i], 32);
-            mbar_init(&s_empty[i], kConsumerWarps);
-        }
-        mbar_fence_init();
-    }
-    for (int it = tid; it < G * (kU + 1); it += kZpThreads) {
-        const int g = it / (kU + 1), q0 = it - g * (kU + 1);
-        const DevView &V = view_of(g);
-        const int q = u0 + min(q0, nu);
-        const double lx = det[t.off_bx + q], ly = det[t.off_by + q];
-        const double wx = lx * V.c - ly * V.s, wy = lx * V.s + ly * V.c;
-        const double wa = V.xdrv ? wx : wy, wb = V.xdrv ? wy : wx;
-        const double m = (wb - V.Sb) / (wa - V.Sa);
-        s_m[g][q0] = m;
-        s_c0[g][q0] = (V.Sb - V.b_lo) / dx + m * (V.a0 - V.Sa) / dx;
-    }
-    for (int it = tid; it < G * kU; it += kZpThreads) {
-        const int g = it / kU, uq = it - g * kU;
-        const DevView &V = view_of(g);
-        const int u = u0 + min(uq, nu - 1);
-        const double lx = det[t.off_ux + u], ly = det[t.off_uy + u];
-        const double ca = V.xdrv ? (lx * V.c - ly * V.s) : (lx * V.s + ly * V.c);
-        s_r[g][uq] = 1.0 / (ca - V.Sa);
-    }
-    for (int it = tid; it < G * (DNV + 1); it += kZpThreads) {
-        const int g = it / (DNV + 1), w = it - g * (DNV + 1);
-        const DevView &V = view_of(g);
-        s_e[it] = (float)((det[t.off_bz + w] + V.zP - V.Sz) / a.dz);
-    }
-    if (tid < G) {
-        const DevView &V = view_of(tid);
-        s_ga0[tid] = V.a0 - V.Sa;
-        s_Z0[tid] = (float)((V.Sz - a.z_lo) / a.dz);
-    }
-    __syncthreads();
-
-    double r2 = 0.0;
-    if (warp == kConsumerWarps) {
-        // ---------------- producer warp ----------------
-        int issued = 0;
-        for (int j = 0; j < na; ++j) {
-            const int b = j % nbuf;
-            if (j >= nbuf) {
-                bool ok = true;
-                if (lane == 0) ok = mbar_wait(&s_empty[b], (uint32_t)(((j / nbuf) - 1) & 1));
-                ok = __shfl_sync(0xffffffffu, ok, 0);
-                if (!ok) {
-                    if (lane == 0) {
-                        s_abort = 1;
-                        if (a.err) atomicExch(a.err, CTLAB_ERR_TIMEOUT);
-                    }
-                    break;
-                }
-            }
-            if (*(volatile int *)&s_abort) break;
-            // staged column range: union over the group's views of the
-            // tile's outer boundary rays at slice j
-            double xmin = 1e300, xmax = -1e300;
-#pragma unroll
-            for (int g = 0; g < G; ++g) {
-                const double x0 = s_c0[g][0] + s_m[g][0] * (double)j, x1 = s_c0[g][kU] + s_m[g][kU] * (double)j;
-                xmin = fmin(xmin, fmin(x0, x1));
-                xmax = fmax(xmax, fmax(x0, x1));
-            }
-            xmin = fmin(fmax(xmin, 0.0), (double)(nb - 1));
-            xmax = fmin(fmax(xmax, 0.0), (double)(nb - 1));
-            SliceInfo in;
-            in.i_lo = max((int)xmin - 1, 0);
-            in.ncols = min((int)xmax + 1, nb - 1) - in.i_lo + 1;
-            // staged z range: extremes of Z0 + T e over the tile's corners
-            float zmin = 1e30f, zmax = -1e30f;
-#pragma unroll
-            for (int g = 0; g < G; ++g) {
-                const double ga = s_ga0[g] + (double)j * dx;
-                const float Ta = (float)(ga * s_r[g][0]), Tb = (float)(ga * s_r[g][nu - 1]);
-                const float e0 = s_e[g * (DNV + 1)], e1 = s_e[g * (DNV + 1) + DNV];
-                const float Z0 = s_Z0[g];
-                const float c0 = Ta * e0, c1 = Ta * e1, c2 = Tb * e0, c3 = Tb * e1;
-                zmin = fminf(zmin, Z0 + fminf(fminf(c0, c1), fminf(c2, c3)));
-                zmax = fmaxf(zmax, Z0 + fmaxf(fmaxf(c0, c1), fmaxf(c2, c3)));
-            }
-            const float zl = fminf(fmaxf(floorf(zmin) - 1.f, 0.f), (float)(ZN - 1));
-            in.k_lo = (int)zl;
-            const float zh = fminf(fmaxf(floorf(zmax) + 2.f, (float)(in.k_lo + 1)), (float)ZN);
-            in.k_hi = (int)zh;
-            in.k_lo_a = in.k_lo & ~3;
-            in.kcount = min((in.k_hi + 4) & ~3, zp) - in.k_lo_a;
-            in.fits = in.ncols <= cmax;
-            in.pad = 0;
-            // boundary columns and fractions of every view
-            for (int it = lane; it < G * (kU + 1); it += 32) {
-                const int g = it / (kU + 1), q = it - g * (kU + 1);
-                const double x = s_c0[g][q] + s_m[g][q] * (double)j;
-                const double xc = fmin(fmax(x, 0.0), (double)nb);
-                const int i = min((int)xc, nb - 1);
-                const int c = in.fits ? min(max(i - in.i_lo, 0), in.ncols - 1) : i;
-                s_cf[b][g][q] = make_int2(c, __float_as_int((float)(xc - (double)i)));
-            }
-            if (lane == 0) {
-                s_info[b] = in;
-                mbar_arrive_expect_tx(&s_full[b], in.fits ? (uint32_t)(4 * in.ncols * in.kcount) : 0u);
-            }
-            __syncwarp();
-            if (in.fits) {
-                const float *src = sat + (long long)j * s_slice + (long long)in.i_lo * s_col + in.k_lo_a;
-                float *dst = colbuf + (size_t)b * cmax * kstr;
-                for (int c = lane; c < in.ncols; c += 32)
-                    bulk_copy_g2s(dst + (size_t)c * kstr, src + (long long)c * s_col, (uint32_t)(4 * in.kcount),
-                                  &s_full[b]);
-            }
-            if (lane != 0) mbar_arrive(&s_full[b]);
-            issued = j + 1;
-        }
-        // copies still in flight land before the CTA may exit
-        if (lane == 0)
-            for (int j = max(issued - nbuf, 0); j < issued; ++j)
-                if (!mbar_wait(&s_full[j % nbuf], (uint32_t)((j / nbuf) & 1)) && a.err)
-                    atomicExch(a.err, CTLAB_ERR_TIMEOUT);
-    } else {
-        // ---------------- consumer warps ----------------
-        const int uu = warp * 2 + (lane >> 4), vs = lane & 15, v0 = vs * NR;
-        const bool owner = uu < nu && v0 < DNV;
-        const int uq = min(uu, nu - 1);
-        float cT0[G], cdT[G], cW0[G], cdW[G];
-#pragma unroll
-        for (int g = 0; g < G; ++g) {
-            const double r = s_r[g][uq];
-            cT0[g] = (float)(s_ga0[g] * r);
-            cdT[g] = (float)(dx * r);
-            cW0[g] = (float)(s_c0[g][uq + 1] - s_c0[g][uq]);
-            cdW[g] = (float)(s_m[g][uq + 1] - s_m[g][uq]);
-        }
-        float acc[G][NR];
-#pragma unroll
-        for (int g = 0; g < G; ++g)
-#pragma unroll
-            for (int r = 0; r < NR; ++r) acc[g][r] = 0.f;
-
-        for (int j = 0; j < na; ++j) {
-            const int b = j % nbuf;
-            if (!mbar_wait(&s_full[b], (uint32_t)((j / nbuf) & 1))) {
-                if (lane == 0) {
-                    s_abort = 1;
-                    if (a.err) atomicExch(a.err, CTLAB_ERR_TIMEOUT);
-                }
-                break;
-            }
-            const SliceInfo in = s_info[b];
-            const float jf = (float)j;
-            if (owner) {
-                const float *Sb = colbuf + (size_t)b * cmax * kstr - in.k_lo_a;
-                const float *Sg = sat + (long long)j * s_slice;
-                const int klo = in.k_lo, khi1 = in.k_hi - 1;
-#pragma unroll
-                for (int g = 0; g < G; ++g) {
-                    if (s_pos_list[g] < 0) continue;
-                    const int2 ea = s_cf[b][g][uu], eb = s_cf[b][g][uu + 1];
-                    const int ca = ea.x, cb = eb.x, dc = cb - ca;
-                    const float fa = __int_as_float(ea.y), fb = __int_as_float(eb.y);
-                    const float T_ = fmaf(jf, cdT[g], cT0[g]);
-                    const float den = fmaf(jf, cdW[g], cW0[g]) * T_;
-                    const float scale = (den != 0.f) ? __fdividef(1.f, den) : 0.f;
-                    const float Z0 = s_Z0[g];
-                    const float *e = s_e + g * (DNV + 1);
-                    // strip integral at z-boundary coordinate kz
-                    auto strip = [&](float kz) -> float {
-                        kz = fminf(fmaxf(kz, 0.f), (float)ZN);
-                        int k0 = min((int)kz, ZN - 1);
-                        const float fz = kz - (float)k0;
-                        k0 = min(max(k0, klo), khi1);
-                        float Ca0, Ca1, Cb0, Cb1, dS0 = 0.f, dS1 = 0.f;
-                        if (in.fits) {
-                            const float *pa = Sb + ca * kstr + k0, *pb = Sb + cb * kstr + k0;
-                            Ca0 = pa[0]; Ca1 = pa[1]; Cb0 = pb[0]; Cb1 = pb[1];
-                            if (dc == 1) { dS0 = Ca0; dS1 = Ca1; }
-                            else if (dc == -1) { dS0 = -Cb0; dS1 = -Cb1; }
-                            else if (dc != 0) {
-                                const int lo = min(ca, cb), hi = max(ca, cb);
-                                for (int c = lo; c < hi; ++c) { dS0 += Sb[c * kstr + k0]; dS1 += Sb[c * kstr + k0 + 1]; }
-                                if (dc < 0) { dS0 = -dS0; dS1 = -dS1; }
-                            }
-                        } else {
-                            const float *pa = Sg + ca * s_col + k0, *pb = Sg + cb * s_col + k0;
-                            Ca0 = pa[0]; Ca1 = pa[1]; Cb0 = pb[0]; Cb1 = pb[1];
-                            const int lo = min(ca, cb), hi = max(ca, cb);
-                            for (int c = lo; c < hi; ++c) { dS0 += Sg[c * s_col + k0]; dS1 += Sg[c * s_col + k0 + 1]; }
-                            if (dc < 0) { dS0 = -dS0; dS1 = -dS1; }
-                        }
-                        const float D0 = dS0 + (fb * Cb0 - fa * Ca0);
-                        const float D1 = dS1 + (fb * Cb1 - fa * Ca1);
-                        return fmaf(fz, D1 - D0, D0);
-                    };
-                    float dp = strip(fmaf(T_, e[v0], Z0));
-#pragma unroll
-                    for (int r = 0; r < NR; ++r) {
-                        if (v0 + r < DNV) {
-                            const float dn = strip(fmaf(T_, e[v0 + r + 1], Z0));
-                            acc[g][r] = fmaf(dn - dp, scale, acc[g][r]);
-                            dp = dn;
-                        }
-                    }
-                }
-            }
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&s_empty[b]);
-        }
-
-        // epilogue
-#pragma unroll
-        for (int g = 0; g < G; ++g) {
-            const int li = s_pos_list[g];
-            if (li < 0 || !owner) continue;
-            const DevView &V = view_of(g);
-            const int u = u0 + uu;
-            const double lx = det[t.off_ux + u], ly = det[t.off_uy + u];
-            const double cx = lx * V.c - ly * V.s, cy = lx * V.s + ly * V.c;
-            const double ex = cx - V.Sx, ey = cy - V.Sy;
-            const double ea = V.xdrv ? ex : ey;
-#pragma unroll
-            for (int r = 0; r < NR; ++r) {
-                const int v = v0 + r;
-                if (v < DNV) {
-                    const double ez = det[t.off_vz + v] + V.zP - V.Sz;
-                    const double L = dx * sqrt(ex * ex + ey * ey + ez * ez) / fabs(ea);
-                    const double de = (det[t.off_bz + v + 1] - det[t.off_bz + v]) / a.dz;
-                    const float val = (float)((double)acc[g][r] * (L / de));
-                    const long long idx = ((long long)li * a.DNU + u) * DNV + v;
-                    if (a.epilogue == PROJ_SART_RESIDUAL) {
-                        const float mv = a.meas[idx], rs = a.row_sum[idx];
-                        const float res = mv - val;
-                        r2 += (double)res * (double)res;
-                        a.out[idx] = (rs > 1.0e-7f) ? res / rs : 0.f;
-                    } else {
-                        a.out[idx] = val;
-                    }
-                }
-            }
-        }
-    }
-    if (a.epilogue == PROJ_SART_RESIDUAL && a.resid2) {
-        __shared__ double s_red[kConsumerWarps + 1];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) r2 += __shfl_down_sync(0xffffffffu, r2, o);
-        if (lane == 0) s_red[warp] = r2;
-        __syncthreads();
-        if (tid == 0) {
-            double sum = 0.0;
-            for (int w = 0; w <= kConsumerWarps; ++w) sum += s_red[w];
-            atomicAdd(a.resid2, sum);
-        }
-    }
-}
-
-size_t dyn_smem_zp(int cmax, int kstr, int DNV, int G, int nbuf)
-{
-    return 4 * (size_t)nbuf * cmax * kstr + sizeof(float) * (size_t)G * (DNV + 1);
-}
-
-template <int NR, int G>
-cudaError_t launch_zp_g(const ProjArgs &a, cudaStream_t s)
-{
-    const size_t sm = dyn_smem_zp(a.cmax, a.zp, a.DNV, G, a.nbuf);
-    auto kern = dd3_proj_zp_kernel<NR, G>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
-    dim3 grid((a.DNU + kU - 1) / kU, a.ngroups);
-    kern<<<grid, kZpThreads, sm, s>>>(a, a.cmax, a.zp);
-    return cudaGetLastError();
-}
-
-template <int NR>
-cudaError_t launch_zp_nr(const ProjArgs &a, cudaStream_t s)
-{
-    switch (a.G) {
-    case 1: return launch_zp_g<NR, 1>(a, s);
-    case 2: return launch_zp_g<NR, 2>(a, s);
-    case 4: return launch_zp_g<NR, 4>(a, s);
-    default: return cudaErrorInvalidValue;
-    }
-}
-
-cudaError_t launch_zp(const ProjArgs &a, cudaStream_t s)
-{
-    const int need = (a.DNV + 15) / 16;
-    if (need <= 1) return launch_zp_nr<1>(a, s);
-    if (need <= 2) return launch_zp_nr<2>(a, s);
-    if (need <= 4) return launch_zp_nr<4>(a, s);
-    if (need <= 8) return launch_zp_nr<8>(a, s);
-    if (need <= 16) return launch_zp_nr<16>(a, s);
-    return cudaErrorInvalidValue;
-}
-
 size_t dyn_smem(int cmax, int kstr, int ds, int DNV, int G, size_t elem, int nbuf)
 {
     return elem * nbuf * (size_t)cmax * kstr + sizeof(float) * (2 * (size_t)kU * ds + (size_t)G * (DNV + 1));
@@ -862,7 +447,7 @@ cudaError_t launch_nr(const ProjArgs &a, cudaStream_t s)
 template <class T>
 cudaError_t launch_t(const ProjArgs &a, cudaStream_t s)
 {
-    static_assert(sizeof(T) == 4 || sizeof(T) == 8, "SAT element");
+    static_assert(sizeof(T) == 8, "SAT element");
     const int need = (a.DNV + kVS - 1) / kVS;
     if (need <= 1) return launch_nr<1, T>(a, s);
     if (need <= 2) return launch_nr<2, T>(a, s);
@@ -921,10 +506,8 @@ ProjStaging proj_staging(const HostGeometry &g, int zp, int elem_bytes)
     }
     // deepest staging (2..4 slices in flight) whose buffers hold the group
     // span, else the single-view span; CTLAB_PROJ_NBUF overrides the depth
-    const bool zpre = elem_bytes == 4;
     const int ds = (g.ZN + 1) | 1;
-    const size_t fixed = (zpre ? dyn_smem_zp(0, zp, g.DNV, kGMax, 0)
-                               : dyn_smem(0, zp, ds, g.DNV, kGMax, elem_bytes, 0)) + kStaticSmem;
+    const size_t fixed = dyn_smem(0, zp, ds, g.DNV, kGMax, elem_bytes, 0) + kStaticSmem;
     auto cap_of = [&](int nbuf) { return (int)((kSmemLimit - fixed) / ((size_t)elem_bytes * nbuf * (size_t)zp)); };
     int want = 0;
     if (const char *env = std::getenv("CTLAB_PROJ_NBUF")) want = std::atoi(env);
@@ -949,13 +532,8 @@ ProjStaging proj_staging(const HostGeometry &g, int zp, int elem_bytes)
 
 ProjGroups proj_make_groups(const HostGeometry &g, const std::vector<int> &list, int cmax)
 {
-    // positions of the list by driving axis, each ordered by angle
-    std::vector<int> byaxis[2];
-    for (int pos = 0; pos < (int)list.size(); ++pos) byaxis[g.views[list[pos]].xdrv].push_back(pos);
-    for (auto &v : byaxis)
-        std::stable_sort(v.begin(), v.end(), [&](int a, int b) {
-            return std::atan2(g.views[list[a]].s, g.views[list[a]].c) < std::atan2(g.views[list[b]].s, g.views[list[b]].c);
-        });
+    // positions of the list in runs of angularly adjacent views of one axis
+    const std::vector<std::vector<int>> byaxis = view_runs(g, list);
     // CTLAB_PROJ_GMAX (1, 2 or 4) caps the views per CTA; default 4
     int gmax = kGMax;
     if (const char *env = std::getenv("CTLAB_PROJ_GMAX")) {
@@ -967,7 +545,7 @@ ProjGroups proj_make_groups(const HostGeometry &g, const std::vector<int> &list,
         if (G > gmax) continue;
         bool ok = true;
         std::vector<int> table;
-        for (auto &v : byaxis) {
+        for (const auto &v : byaxis) {
             for (size_t i0 = 0; i0 < v.size() && ok; i0 += G) {
                 std::vector<const DevView *> vs;
                 for (int k = 0; k < G; ++k) {
@@ -998,7 +576,6 @@ cudaError_t launch_proj(const ProjArgs &a, cudaStream_t s, int *launches)
     if (a.n <= 0 || a.ngroups <= 0) return cudaSuccess;
     if (a.ngroups > 65535) return cudaErrorInvalidConfiguration;
     if (launches) ++*launches;
-    if (a.zprefix) return launch_zp(a, s);
     return a.f32pair ? launch_t<ff2>(a, s) : launch_t<double>(a, s);
 }
 

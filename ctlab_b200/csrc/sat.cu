@@ -338,54 +338,64 @@ cudaError_t launch_volume_sat(const float *vol, const unsigned char *mask, int X
 
 namespace {
 
-// One warp per voxel column: each lane sums a contiguous run of the column
-// in FP64, a warp-shuffle scan turns the lane totals into offsets, and the
-// lanes write their running sums rounded to FP32.
-__global__ void __launch_bounds__(256) zprefix_kernel(const float *__restrict__ vol, const unsigned char *mask,
-                                                      long long ncols, int ZN, float *__restrict__ out, int zpc)
+// Slice-major z-prefixes: one CTA per 32 columns of one slice.  Each warp
+// scans 4 columns 32 rows at a time (coalesced loads along z, FP64 warp
+// scan plus a carried FP64 total), the rounded prefixes go through a padded
+// shared tile, and the CTA writes them out as rows of 32 adjacent columns.
+__global__ void __launch_bounds__(256) zt_kernel(const float *__restrict__ vol, const unsigned char *mask, int XN,
+                                                 int ZN, int nb, int orientation, float *__restrict__ out, int rs)
 {
-    const int lane = threadIdx.x & 31;
-    const long long col = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (col >= ncols) return;
-    const float m = mask ? (mask[col] ? 1.f : 0.f) : 1.f;
-    const float *in = vol + col * ZN;
-    float *o = out + col * zpc;
-    const int per = (ZN + 31) >> 5;
-    const int k0 = lane * per;
-    double tot = 0.0;
-    for (int r = 0; r < per; ++r) {
-        const int k = k0 + r;
-        if (k < ZN) tot += (double)(__ldg(in + k) * m);
-    }
-    double incl = tot;
+    __shared__ float tile[32][33];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int j = blockIdx.y, c0 = blockIdx.x * 32;
+    const float *col[4];
+    float m[4];
+    double carry[4];
 #pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const double y = __shfl_up_sync(kFull, incl, d);
-        if (lane >= d) incl += y;
+    for (int i = 0; i < 4; ++i) {
+        const int c = c0 + warp * 4 + i;
+        const bool valid = c < nb;
+        const int x = orientation ? j : c, y = orientation ? c : j;
+        const long long ci = valid ? (long long)y * XN + x : 0;
+        col[i] = vol + ci * ZN;
+        m[i] = valid ? (mask ? (mask[ci] ? 1.f : 0.f) : 1.f) : 0.f;
+        carry[i] = 0.0;
     }
-    double run = __shfl_up_sync(kFull, incl, 1);
-    if (lane == 0) {
-        run = 0.0;
-        o[0] = 0.f;
-    }
-    for (int r = 0; r < per; ++r) {
-        const int k = k0 + r;
-        if (k < ZN) {
-            run += (double)(__ldg(in + k) * m);
-            o[k + 1] = (float)run;
+    float *plane = out + (long long)j * (ZN + 1) * rs;
+    const int cw = c0 + lane;
+    if (warp == 0 && cw < rs) plane[cw] = 0.f; // row 0
+    for (int z0 = 0; z0 < ZN; z0 += 32) {
+        const int z = z0 + lane;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            double v = (z < ZN && m[i] != 0.f) ? (double)(__ldg(col[i] + z) * m[i]) : 0.0;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const double y = __shfl_up_sync(kFull, v, d);
+                if (lane >= d) v += y;
+            }
+            v += carry[i];
+            tile[lane][warp * 4 + i] = (float)v;
+            carry[i] = __shfl_sync(kFull, v, 31);
         }
+        __syncthreads();
+        for (int rr = warp; rr < 32; rr += 8) {
+            const int k = z0 + 1 + rr;
+            if (k <= ZN && cw < rs) plane[(long long)k * rs + cw] = cw < nb ? tile[rr][lane] : 0.f;
+        }
+        __syncthreads();
     }
 }
 
 } // namespace
 
-cudaError_t launch_zprefix(const float *vol, const unsigned char *mask, int XN, int YN, int ZN, float *out, int zpc,
-                           cudaStream_t s)
+cudaError_t launch_zt(const float *vol, const unsigned char *mask, int XN, int YN, int ZN, int orientation,
+                      float *out, int rs, cudaStream_t s)
 {
-    const long long ncols = (long long)XN * YN;
-    const long long blocks = (ncols * 32 + 255) / 256;
-    if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
-    zprefix_kernel<<<(unsigned)blocks, 256, 0, s>>>(vol, mask, ncols, ZN, out, zpc);
+    const int nb = orientation ? YN : XN, na = orientation ? XN : YN;
+    if (rs < nb || na > 65535) return cudaErrorInvalidValue;
+    dim3 grid((rs + 31) / 32, na);
+    zt_kernel<<<grid, 256, 0, s>>>(vol, mask, XN, ZN, nb, orientation, out, rs);
     return cudaGetLastError();
 }
 

@@ -49,10 +49,10 @@ extern "C" {
 /* Summed-area-table arithmetic of a plan.  FP64: 2-D FP64 prefix sums of the
  * volume slices and projections; F32PAIR: the same as compensated FP32 pairs
  * (hi+lo float-float sums); both 8 bytes per entry.  ZPREFIX: the projector
- * stages per-column z prefix sums (FP64 sums rounded to FP32, 4 bytes, one
- * array for both driving axes) and forms the in-plane integral from adjacent
- * columns -- the same FP32 quantities the 2-D FP64 path forms after its
- * column differences; the backprojector keeps FP64 projection SATs. */
+ * stages per-column z prefix sums (FP64 sums rounded to FP32, 4 bytes),
+ * slice-major per driving axis, and forms the in-plane integral from
+ * adjacent columns -- the same FP32 quantities the 2-D FP64 path forms after
+ * its column differences; the backprojector keeps FP64 projection SATs. */
 #define CTLAB_SAT_FP64 0
 #define CTLAB_SAT_F32PAIR 1
 #define CTLAB_SAT_ZPREFIX 2
@@ -163,7 +163,9 @@ int ctlab_volume_sat_noalloc(const float *d_vol, const unsigned char *d_mask, in
 /* Copies the plan's volume SAT of one orientation to d_out (FP64 plans:
  * doubles, [planes][rows][zp] as reported by ctlab_plan_sat_layout;
  * F32PAIR plans: float pairs (hi, lo) with the same indexing; ZPREFIX plans:
- * floats [YN][XN][zp] column z-prefixes, either orientation). */
+ * floats [planes][rows][zp] = slice-major column z-prefixes, [YN][ZN+1][rs]
+ * (x fastest) for orientation 0 and [XN][ZN+1][rs] (y fastest) for 1, rs the
+ * row stride reported as zp, pad columns zero). */
 int ctlab_plan_sat_layout(const ctlab_plan *plan, int orientation, int *planes, int *rows,
                           int *zp);
 int ctlab_copy_volume_sat(ctlab_plan *plan, int orientation, void *d_out, void *stream);

@@ -98,6 +98,28 @@ def test_backprojection_matches_oracle(torch_cuda, name, sat_mode):
     assert err <= REL_L2, f"{name}: rel L2 {err:.3e}"
 
 
+@pytest.mark.parametrize("name", ["small", "coarse_det", "odd_offsets"])
+@pytest.mark.parametrize("env", [{"CTLAB_PROJT_CBMAX": "8"}, {"CTLAB_PROJT_GMAX": "1", "CTLAB_PROJT_NSTAGE": "2"},
+                                 {"CTLAB_PROJT_GMAX": "2", "CTLAB_PROJT_NSTAGE": "4"}])
+def test_zprefix_projector_staging_variants_match_oracle(torch_cuda, name, env, monkeypatch):
+    """Stage capacities that force the global-memory fallback (8 staged columns)
+    and other view-group sizes / stage depths of the z-prefix projector."""
+    torch = torch_cuda
+    for k, v in env.items():
+        monkeypatch.setenv(k, v)
+    g = make_case(name)
+    vol = phantom(g)
+    ref = oracle.dd3_proj(g, vol)
+    with cb.Plan(g, sat_mode=cb.CTLAB_SAT_ZPREFIX) as plan:
+        out = torch.zeros(g.prj_shape, dtype=torch.float32, device="cuda")
+        plan.proj(dev(torch, vol), out)
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+    err = rel_l2(got, ref)
+    record_error(f"proj/{name}/zprefix/{'_'.join(env.values())}", err)
+    assert err <= REL_L2, f"{name} {env}: rel L2 {err:.3e}"
+
+
 def test_volume_sat_matches_oracle(torch_cuda):
     torch = torch_cuda
     g = G.small(PN=8, XN=70, YN=45, ZN=33, start=0.0)  # both orientations present
@@ -121,18 +143,21 @@ def test_volume_sat_matches_oracle(torch_cuda):
                 s = s[:, :, : g.ZN + 1]
                 assert s.shape == ref.shape
                 np.testing.assert_allclose(s, ref, rtol=tol, atol=tol * np.abs(ref).max())
-    # column z-prefixes (ZPREFIX plans): FP64 sums rounded to FP32
+    # slice-major column z-prefixes (ZPREFIX plans): FP64 sums rounded to FP32,
+    # [y][k][x] for y slices and [x][k][y] for x slices
     masked = vol.astype(np.float64) * mask.reshape(g.YN, g.XN, 1)
-    zref = np.concatenate([np.zeros((g.YN, g.XN, 1)), np.cumsum(masked, axis=2)], axis=2)
+    zref = np.concatenate([np.zeros((g.YN, g.XN, 1)), np.cumsum(masked, axis=2)], axis=2)  # [y][x][k]
     with cb.Plan(g, sat_mode=cb.CTLAB_SAT_ZPREFIX) as plan:
         plan.volume_sat(dev(torch, vol), dev(torch, mask))
-        planes, rows, zp = plan.sat_layout(0)
-        assert (planes, rows) == (g.YN, g.XN) and zp >= g.ZN + 1
-        buf = torch.zeros(planes * rows * zp, dtype=torch.float32, device="cuda")
-        plan.copy_volume_sat(0, buf)
-        torch.cuda.synchronize()
-        zs = buf.cpu().numpy().reshape(planes, rows, zp)[:, :, : g.ZN + 1]
-        np.testing.assert_allclose(zs, zref, rtol=1e-6, atol=1e-7 * np.abs(zref).max())
+        for o, ref in ((0, zref.transpose(0, 2, 1)), (1, zref.transpose(1, 2, 0))):
+            planes, rows, rs = plan.sat_layout(o)
+            assert (planes, rows) == ref.shape[:2] and rs >= ref.shape[2] and rs % 4 == 0
+            buf = torch.full((planes * rows * rs,), 7.0, dtype=torch.float32, device="cuda")
+            plan.copy_volume_sat(o, buf)
+            torch.cuda.synchronize()
+            zs = buf.cpu().numpy().reshape(planes, rows, rs)
+            np.testing.assert_allclose(zs[:, :, : ref.shape[2]], ref, rtol=1e-6, atol=1e-7 * np.abs(ref).max())
+            assert not zs[:, :, ref.shape[2]:].any()  # pad columns are zero
 
 
 def test_config1_views_match_oracle(torch_cuda):
