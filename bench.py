@@ -42,12 +42,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--sat", default="fp64", choices=["fp64", "f32pair", "zprefix"])
+    ap.add_argument("--sat", default="zprefix", choices=["fp64", "f32pair", "zprefix"])
     ap.add_argument("--cpu-views", type=int, default=4, help="views in the bounded CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--views", type=int, default=0,
-                    help="profiling case: keep only this many evenly spaced views of the 984 (0 = all)")
+                    help="profiling case: keep only this many of the 984 views, in evenly spaced runs of 8 "
+                         "adjacent views (0 = all)")
     return ap.parse_args()
 
 
@@ -55,7 +56,10 @@ def workload_geometry(args):
     from ctlab_b200 import geometry as G
     g = G.config2()
     if args.views:
-        g = g.with_views(np.linspace(0, g.PN - 1, args.views).round().astype(int))
+        runs = max(1, args.views // 8)
+        starts = np.linspace(0, g.PN - 8, runs).round().astype(int)
+        idx = np.unique(np.concatenate([s + np.arange(8) for s in starts]))[: args.views]
+        g = g.with_views(idx)
     return g
 
 
@@ -208,6 +212,7 @@ def run_ours(args):
     hx, hy, hz = G.half_extents(g)
     ell = cb.random_ellipsoids(1 + rank, hx, hy, hz)
     sat_mode = {"fp64": cb.CTLAB_SAT_FP64, "f32pair": cb.CTLAB_SAT_F32PAIR, "zprefix": cb.CTLAB_SAT_ZPREFIX}[args.sat]
+    os.environ["CTLAB_LEGACY_SAT"] = str(sat_mode)  # the e2e arm's DD3Proj_gpu / DD3Back_gpu use the same SAT
     plan = cb.Plan(g, device=local, sat_mode=sat_mode)
     vol = torch.zeros(g.vol_shape, dtype=torch.float32, device="cuda")
     cb.ellipsoid_phantom(vol, g, ell)

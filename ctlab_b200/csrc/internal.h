@@ -178,7 +178,8 @@ struct ProjArgs {
     const float *zt_y, *zt_x; // [YN][ZN+1][zt_rs_y], [XN][ZN+1][zt_rs_x]
     int zt_rs_y, zt_rs_x;
     int t_cb, t_kb, t_kr;     // stage: [t_kr][t_cb] floats, TMA boxes of t_kb rows
-    int t_nstage, t_nw, t_ep, t_gtab;
+    int t_nstage, t_rb, t_ep, t_gtab; // stages, consumer warps per view, z-boundary pitch, table views
+    int t_zs;                         // detector rows split over t_zs CTAs
 };
 
 // Views of one launch grouped by driving axis and angle, G per CTA.
@@ -195,12 +196,13 @@ struct ProjStaging {
 };
 ProjStaging proj_staging(const HostGeometry &g, int zp, int elem_bytes);
 
-// Staging of the slice-major z-prefix projector: G views per CTA, NR
-// detector rows per consumer warp (NW warps), stages of KR rows x CB
+// Staging of the slice-major z-prefix projector: up to G views per CTA, the
+// detector rows split over ZS CTAs, RB consumer warps of NR detector rows
+// per view, stages of KR rows x CB
 // columns (TMA boxes of KB rows), nstage stages, EP floats per view of
 // detector z boundaries.
 struct ProjTStaging {
-    int G = 1, NR = 1, NW = 1, CB = 0, KB = 0, KR = 0, nstage = 2, EP = 4;
+    int G = 1, NR = 4, RB = 1, ZS = 1, CB = 0, KB = 0, KR = 0, nstage = 2, EP = 8;
     size_t smem = 0;
     bool ok = false;
 };

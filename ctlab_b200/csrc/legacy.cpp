@@ -7,6 +7,7 @@
 // when the geometry changes, buffers only grow), so repeated calls with one
 // scan geometry pay no allocation.  Calls on one device are serialised.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <random>
@@ -90,7 +91,15 @@ int legacy_prepare(LegacyCtx &c, const ctlab_geometry &g, int gpunum)
     if (!c.plan || c.key != key) {
         if (c.plan) ctlab_plan_destroy(c.plan);
         c.plan = nullptr;
-        int rc = ctlab_plan_create(&g, gpunum, CTLAB_SAT_FP64, &c.plan);
+        // SAT arithmetic of the cached plan: slice-major FP64-accumulated
+        // z-prefixes unless CTLAB_LEGACY_SAT selects 0 (2-D FP64 SAT) or 1
+        // (compensated FP32 pairs)
+        int mode = CTLAB_SAT_ZPREFIX;
+        if (const char *env = std::getenv("CTLAB_LEGACY_SAT")) {
+            const int m = std::atoi(env);
+            if (m == CTLAB_SAT_FP64 || m == CTLAB_SAT_F32PAIR || m == CTLAB_SAT_ZPREFIX) mode = m;
+        }
+        int rc = ctlab_plan_create(&g, gpunum, mode, &c.plan);
         if (rc != CTLAB_OK) return rc;
         c.key = key;
     }

@@ -168,7 +168,8 @@ int plan_proj_list(ctlab_plan *p, const int *d_list, int n, const GroupTab &gt, 
         a.t_kb = st.KB;
         a.t_kr = st.KR;
         a.t_nstage = st.nstage;
-        a.t_nw = st.NW;
+        a.t_rb = st.RB;
+        a.t_zs = st.ZS;
         a.t_ep = st.EP;
         a.t_gtab = st.G;
         cudaError_t e = launch_proj_t(a, st, p->tm_y, p->tm_x, s, &p->last_launches);

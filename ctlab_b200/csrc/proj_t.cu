@@ -14,17 +14,19 @@
 //
 // One CTA owns 32 detector columns (one per lane) of a group of G views of
 // one driving axis with adjacent angles and sweeps the slices.
-//   producer warp  per slice j, every lane maps the two boundary rays of its
-//                  detector column onto slice j for every view of the group
-//                  in FP64: SAT columns and fractions -> the strip weights,
+//   producer warp  per slice j, one lane per view maps the tile's two outer
+//                  boundary rays onto slice j (FP64) and bounds the
+//                  magnification over the tile's columns; a warp reduction
+//                  gives the columns and z rows the group touches, and 3-D
+//                  TMA tile loads (one per <= 256 rows) bring that
+//                  [rows][columns] block into a ring of stages, completed on
+//                  a "full" mbarrier;
+//   consumer warps one warp per (view, block of NR detector rows), lanes =
+//                  detector columns.  Per slice each lane maps its column's
+//                  two boundary rays onto the slice (FP64, while the copy is
+//                  in flight): SAT columns and fractions -> strip weights,
 //                  the central-ray magnification T and 1/(W T) (W the strip
-//                  width in columns); a warp reduction gives the columns and
-//                  z rows the group touches; one 3-D TMA tile load per 256
-//                  rows brings that [rows][columns] block into a ring of
-//                  stages, completed on a "full" mbarrier together with the
-//                  per-view tables;
-//   consumer warps lanes = detector columns, warp w = NR detector rows.  For
-//                  each of the NR+1 z boundaries e_w of its rows,
+//                  width in columns).  For each of the NR+1 z boundaries e_w,
 //                      kz = Z0 + T e_w,
 //                      F(kz) = wa Za(kz) + wb Zb(kz) [+ whole columns between],
 //                  Zc(kz) the column prefix interpolated in z, and
@@ -32,19 +34,18 @@
 //                  Lanes read neighbouring columns of nearly the same rows,
 //                  so the shared-memory loads are free of bank conflicts.
 //                  Each warp hands the stage back on an "empty" mbarrier.
-// floor(kz) comes from the round-toward-zero add of 2^23, so the inner loop
-// issues no float/int conversions.  Slices whose block exceeds a stage read
-// the z-prefixes from global memory instead.  Epilogue: central-ray slab
-// length L = dx |C - S| / |C_a - S_a|, 1/(e_{v+1} - e_v), and optionally the
-// SART residual (b - Ax)/rowSum with a residual reduction.
+// floor(kz) comes from the round-toward-zero add of 2^23 and the biased
+// result feeds the shared-memory address directly, so the inner loop issues
+// no float/int conversions.  Slices whose block exceeds a stage read the
+// z-prefixes from global memory instead.  Epilogue: central-ray slab length
+// L = dx |C - S| / |C_a - S_a|, 1/(e_{v+1} - e_v), and optionally the SART
+// residual (b - Ax)/rowSum with a residual reduction.
 #include <cuda.h>
 
 #include <algorithm>
 #include <climits>
 #include <cmath>
 #include <cstdlib>
-#include <type_traits>
-#include <utility>
 
 #include "internal.h"
 #include "tma.cuh"
@@ -53,14 +54,15 @@ namespace ctlab {
 
 namespace {
 
-constexpr int kTU = 32;          // detector columns per CTA (one per lane)
+constexpr int kTU = 32;           // detector columns per CTA (one per lane)
 constexpr int kTMaxStage = 4;
-constexpr int kTMaxWarps = 8;    // consumer warps
-constexpr int kTMaxG = 8;
+constexpr int kTMaxCWarps = 16;   // consumer warps
+constexpr int kTMaxG = 16;        // views per CTA
+constexpr int kTMaxThreads = (kTMaxCWarps + 1) * 32;
 constexpr size_t kTSmemLimit = 227 * 1024;
-constexpr size_t kTStatic = 10 * 1024; // static shared arrays, rounded up
+constexpr size_t kTStatic = 14 * 1024; // static shared arrays, rounded up
 
-struct __align__(16) TEntry {
+struct TEntry {
     float T, scale, wa, wb;
 };
 struct TSlice {
@@ -69,41 +71,41 @@ struct TSlice {
     int pad0, pad1;
 };
 
-// f(integral_constant<int, 0>) ... f(integral_constant<int, N-1>): a loop
-// whose index is a compile-time constant in the body (register arrays).
-template <class F, int... I>
-__device__ __forceinline__ void static_for_impl(F &&f, std::integer_sequence<int, I...>)
+__device__ __forceinline__ float lds_f32(uint32_t addr)
 {
-    (f(std::integral_constant<int, I>()), ...);
+    float v;
+    asm("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr));
+    return v;
 }
-template <int N, class F>
-__device__ __forceinline__ void static_for(F &&f)
+__device__ __forceinline__ float4 lds_f32x4(uint32_t addr)
 {
-    static_for_impl(f, std::make_integer_sequence<int, N>());
+    float4 v;
+    asm("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(addr));
+    return v;
 }
 
-template <int NR, int G>
-__global__ void __launch_bounds__((kTMaxWarps + 1) * 32, 1)
+template <int NR>
+__global__ void __launch_bounds__(kTMaxThreads, 1)
     dd3_proj_t_kernel(ProjArgs a, const __grid_constant__ CUtensorMap tm_y, const __grid_constant__ CUtensorMap tm_x)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     // TMA destinations need 128-byte alignment (the launch adds 128 bytes)
     unsigned char *smem = smem_raw + ((128 - (smem_addr(smem_raw) & 127)) & 127);
-    const int NW = a.t_nw, nstage = a.t_nstage;
+    const int G = a.G, RB = a.t_rb, NWC = G * RB;
+    const int vbase = blockIdx.z * RB * NR; // first detector row of this CTA (rows split over grid z)
+    const int nstage = a.t_nstage;
     const int CB = a.t_cb, KB = a.t_kb, KR = a.t_kr, EP = a.t_ep, GT = a.t_gtab;
     const int stage_floats = KR * CB;
-    float *stage0 = reinterpret_cast<float *>(smem);                                 // [nstage][KR][CB]
-    TEntry *s_tab = reinterpret_cast<TEntry *>(smem + 4 * stage_floats * nstage);    // [nstage][GT][32]
-    int2 *s_cd = reinterpret_cast<int2 *>(s_tab + nstage * GT * kTU);                // [nstage][GT][32]
-    float *s_e = reinterpret_cast<float *>(s_cd + nstage * GT * kTU);                // [G][EP]
+    float *stage0 = reinterpret_cast<float *>(smem);                    // [nstage][KR][CB]
+    float *s_e = reinterpret_cast<float *>(smem + 4 * stage_floats * nstage); // [GT][EP]
     __shared__ __align__(8) uint64_t s_full[kTMaxStage], s_empty[kTMaxStage];
     __shared__ TSlice s_info[kTMaxStage];
-    __shared__ double s_c0[G][kTU + 1], s_m[G][kTU + 1], s_r[G][kTU];
-    __shared__ double s_ga0[G];
-    __shared__ float s_Z0[G], s_emin[G], s_emax[G];
-    __shared__ int s_pos_list[G];
+    __shared__ double s_c0[kTMaxG][kTU + 1], s_m[kTMaxG][kTU + 1], s_r[kTMaxG][kTU];
+    __shared__ double s_ga0[kTMaxG], s_rmin[kTMaxG], s_rmax[kTMaxG];
+    __shared__ float s_Z0[kTMaxG], s_emin[kTMaxG], s_emax[kTMaxG];
+    __shared__ int s_pos_list[kTMaxG];
     __shared__ int s_abort;
-    __shared__ double s_red[kTMaxWarps + 1];
+    __shared__ double s_red[kTMaxCWarps + 1];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid < G) s_pos_list[tid] = a.groups[blockIdx.y * G + tid];
@@ -117,17 +119,17 @@ __global__ void __launch_bounds__((kTMaxWarps + 1) * 32, 1)
     __syncthreads();
     const DevView &V0 = a.views[a.view_list[s_pos_list[0]]]; // all views of the group share the axis
     const int na = V0.na, nb = V0.nb, xdrv = V0.xdrv;
-    const float *zt = xdrv ? a.zt_x : a.zt_y;
-    const int zrs = xdrv ? a.zt_rs_x : a.zt_rs_y;
     auto view_of = [&](int g) -> const DevView & {
         const int ps = s_pos_list[g] >= 0 ? s_pos_list[g] : s_pos_list[0];
         return a.views[a.view_list[ps]];
     };
 
     if (tid == 0) {
+        int nact = 0;
+        for (int g = 0; g < G; ++g) nact += s_pos_list[g] >= 0;
         for (int i = 0; i < nstage; ++i) {
             mbar_init(&s_full[i], 32);
-            mbar_init(&s_empty[i], NW);
+            mbar_init(&s_empty[i], nact * RB); // one arrival per working consumer warp
         }
         mbar_fence_init();
     }
@@ -153,10 +155,11 @@ __global__ void __launch_bounds__((kTMaxWarps + 1) * 32, 1)
         const double ca = V.xdrv ? (lx * V.c - ly * V.s) : (lx * V.s + ly * V.c);
         s_r[g][uq] = 1.0 / (ca - V.Sa);
     }
-    // detector z boundaries in SAT-row units, relative to the source; rows
-    // past DNV repeat the last boundary (their cells are never stored)
+    // detector z boundaries of this CTA's rows in SAT-row units, relative to
+    // the source; rows past DNV repeat the last boundary (never stored)
+    const int nw_local = min(RB * NR, DNV - vbase); // rows of this CTA
     for (int it = tid; it < G * EP; it += nthreads) {
-        const int g = it / EP, w = min(it - g * EP, DNV);
+        const int g = it / EP, w = min(vbase + it - g * EP, DNV);
         const DevView &V = view_of(g);
         s_e[it] = (float)((det[t.off_bz + w] + V.zP - V.Sz) / a.dz);
     }
@@ -168,17 +171,24 @@ __global__ void __launch_bounds__((kTMaxWarps + 1) * 32, 1)
     __syncthreads();
     if (tid < G) {
         float lo = 1e30f, hi = -1e30f;
-        for (int w = 0; w <= DNV; ++w) {
+        for (int w = 0; w <= nw_local; ++w) {
             lo = fminf(lo, s_e[tid * EP + w]);
             hi = fmaxf(hi, s_e[tid * EP + w]);
         }
         s_emin[tid] = lo;
         s_emax[tid] = hi;
+        double rlo = 1e300, rhi = -1e300; // 1/(C_a - S_a) over the tile's columns
+        for (int uq = 0; uq < nu; ++uq) {
+            rlo = fmin(rlo, s_r[tid][uq]);
+            rhi = fmax(rhi, s_r[tid][uq]);
+        }
+        s_rmin[tid] = rlo;
+        s_rmax[tid] = rhi;
     }
     __syncthreads();
 
     double r2 = 0.0;
-    if (warp == NW) {
+    if (warp == NWC) {
         // ------------------------------ producer ------------------------------
         const CUtensorMap *tm = xdrv ? &tm_x : &tm_y;
         const int uq = min(lane, nu - 1);
@@ -201,44 +211,25 @@ __global__ void __launch_bounds__((kTMaxWarps + 1) * 32, 1)
             const double jd = (double)j;
             int cmin = INT_MAX, cmax = INT_MIN;
             float kmin = 1e30f, kmax = -1e30f;
-            int ia_g[G], dc_g[G];
-            TEntry te_g[G];
-#pragma unroll
-            for (int g = 0; g < G; ++g) {
-                const double xa = fma(s_m[g][uq], jd, s_c0[g][uq]);
-                const double xb = fma(s_m[g][uq + 1], jd, s_c0[g][uq + 1]);
-                const double xac = fmin(fmax(xa, 0.0), (double)nb), xbc = fmin(fmax(xb, 0.0), (double)nb);
-                const int ia = min((int)xac, nb - 1), ib = min((int)xbc, nb - 1);
-                const float fa = (float)(xac - (double)ia), fb = (float)(xbc - (double)ib);
-                const double T = (s_ga0[g] + jd * dx) * s_r[g][uq];
-                const double den = (xb - xa) * T;
-                const int dc = ib - ia;
-                TEntry te;
-                te.T = (float)T;
-                te.scale = (den != 0.0) ? (float)(1.0 / den) : 0.f;
-                if (dc == 0) {
-                    te.wa = fb - fa;
-                    te.wb = 0.f;
-                } else if (dc > 0) {
-                    te.wa = 1.f - fa;
-                    te.wb = fb;
-                } else {
-                    te.wa = -fa;
-                    te.wb = fb - 1.f;
-                }
-                te_g[g] = te;
-                ia_g[g] = ia;
-                dc_g[g] = dc;
-                cmin = min(cmin, min(ia, ib));
-                cmax = max(cmax, max(ia, ib));
-                // z rows of the group: the consumers' kz = fma(T, e, Z0) is
-                // monotone in e, so the extremes of e bound it exactly
-                const float z0 = s_Z0[g];
-                float k0 = fmaf(te.T, s_emin[g], z0), k1 = fmaf(te.T, s_emax[g], z0);
-                k0 = fminf(fmaxf(k0, 0.f), (float)ZN);
-                k1 = fminf(fmaxf(k1, 0.f), (float)ZN);
-                kmin = fminf(kmin, fminf(k0, k1));
-                kmax = fmaxf(kmax, fmaxf(k0, k1));
+            for (int g = lane; g < G; g += 32) {
+                // the outer boundary rays bound the tile's columns (boundary
+                // positions are monotone along the detector); one column of
+                // margin for rounding between them and the interior rays
+                const double x0 = fma(s_m[g][0], jd, s_c0[g][0]), x1 = fma(s_m[g][nu], jd, s_c0[g][nu]);
+                const int i0 = min((int)fmin(fmax(x0, 0.0), (double)nb), nb - 1);
+                const int i1 = min((int)fmin(fmax(x1, 0.0), (double)nb), nb - 1);
+                cmin = min(cmin, max(min(i0, i1) - 1, 0));
+                cmax = max(cmax, min(max(i0, i1) + 1, nb - 1));
+                // the consumers' kz = fma((float)(t r_u), e, Z0) is monotone in
+                // r_u and in e, so the extremes of both bound it exactly
+                const double tj = s_ga0[g] + jd * dx;
+                const float Ta = (float)(tj * s_rmin[g]), Tb = (float)(tj * s_rmax[g]);
+                const float z0 = s_Z0[g], e0 = s_emin[g], e1 = s_emax[g];
+                const float c0 = fmaf(Ta, e0, z0), c1 = fmaf(Ta, e1, z0), c2 = fmaf(Tb, e0, z0), c3 = fmaf(Tb, e1, z0);
+                const float lo = fminf(fmaxf(fminf(fminf(c0, c1), fminf(c2, c3)), 0.f), (float)ZN);
+                const float hi = fminf(fmaxf(fmaxf(fmaxf(c0, c1), fmaxf(c2, c3)), 0.f), (float)ZN);
+                kmin = fminf(kmin, lo);
+                kmax = fmaxf(kmax, hi);
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
@@ -255,11 +246,6 @@ __global__ void __launch_bounds__((kTMaxWarps + 1) * 32, 1)
             const int nk = k_top - k_lo + 1;
             const bool fits = CB > 0 && (cmax - c_lo + 1 <= CB) && (nk <= KR);
             const int nbox = fits ? (nk + KB - 1) / KB : 0;
-#pragma unroll
-            for (int g = 0; g < G; ++g) {
-                s_tab[(b * GT + g) * kTU + lane] = te_g[g];
-                s_cd[(b * GT + g) * kTU + lane] = make_int2(fits ? ia_g[g] - c_lo : ia_g[g], dc_g[g]);
-            }
             if (lane == 0) {
                 TSlice in;
                 in.c_lo = c_lo;
@@ -274,8 +260,7 @@ __global__ void __launch_bounds__((kTMaxWarps + 1) * 32, 1)
             }
             __syncwarp();
             if (lane < nbox)
-                tma_load_3d(stage0 + b * stage_floats + lane * KB * CB, tm, c_lo, k_lo + lane * KB, j,
-                            &s_full[b]);
+                tma_load_3d(stage0 + b * stage_floats + lane * KB * CB, tm, c_lo, k_lo + lane * KB, j, &s_full[b]);
             if (lane != 0) mbar_arrive(&s_full[b]);
             issued = j + 1;
         }
@@ -284,17 +269,46 @@ __global__ void __launch_bounds__((kTMaxWarps + 1) * 32, 1)
             for (int j = max(issued - nstage, 0); j < issued; ++j)
                 if (!mbar_wait(&s_full[j % nstage], (uint32_t)((j / nstage) & 1)) && a.err)
                     atomicExch(a.err, CTLAB_ERR_TIMEOUT);
-    } else {
+    } else if (warp < NWC && s_pos_list[warp / RB] >= 0) {
         // ------------------------------ consumers -----------------------------
-        const int v0 = warp * NR;
-        float acc[G][NR];
+        const int g = warp / RB, v0l = (warp - g * RB) * NR, v0 = vbase + v0l;
+        const float *zt = xdrv ? a.zt_x : a.zt_y;
+        const int zrs = xdrv ? a.zt_rs_x : a.zt_rs_y;
+        const float z0 = s_Z0[g];
+        const uint32_t e_addr = smem_addr(s_e + g * EP + v0l); // 16-byte aligned (EP, v0l multiples of 4)
+        const uint32_t stage_addr = smem_addr(stage0);
+        const uint32_t RS4 = 4u * (uint32_t)CB;
+        // this lane's boundary rays x(q, j) = c0 + m j and 1/(C_a - S_a)
+        const double ma = s_m[g][lane], ca0 = s_c0[g][lane], mb = s_m[g][lane + 1], cb0 = s_c0[g][lane + 1];
+        const double ru = s_r[g][min(lane, nu - 1)], ga0 = s_ga0[g];
+        const double nbd = (double)nb;
+        float acc[NR];
 #pragma unroll
-        for (int g = 0; g < G; ++g)
-#pragma unroll
-            for (int r = 0; r < NR; ++r) acc[g][r] = 0.f;
+        for (int r = 0; r < NR; ++r) acc[r] = 0.f;
 
         for (int j = 0; j < na; ++j) {
             const int b = j % nstage;
+            // this column's strip on slice j (FP64 positions, FP32 weights)
+            const double jd = (double)j;
+            const double xa = fma(ma, jd, ca0), xb = fma(mb, jd, cb0);
+            const double xac = fmin(fmax(xa, 0.0), nbd), xbc = fmin(fmax(xb, 0.0), nbd);
+            const int ia = min((int)xac, nb - 1), ib = min((int)xbc, nb - 1);
+            const float fa = (float)(xac - (double)ia), fb = (float)(xbc - (double)ib);
+            TEntry te;
+            te.T = (float)((ga0 + jd * dx) * ru);
+            const float den = (float)(xb - xa) * te.T;
+            te.scale = (den != 0.f) ? __frcp_rn(den) : 0.f;
+            const int dc = ib - ia; // column b = column a + dc
+            if (dc == 0) {
+                te.wa = fb - fa;
+                te.wb = 0.f;
+            } else if (dc > 0) {
+                te.wa = 1.f - fa;
+                te.wb = fb;
+            } else {
+                te.wa = -fa;
+                te.wb = fb - 1.f;
+            }
             if (!mbar_wait(&s_full[b], (uint32_t)((j / nstage) & 1))) {
                 if (lane == 0) {
                     s_abort = 1;
@@ -303,98 +317,110 @@ __global__ void __launch_bounds__((kTMaxWarps + 1) * 32, 1)
                 break;
             }
             const TSlice in = s_info[b];
-            // one slice of one view g; GLB: the block is read from global memory
-            auto slice_view = [&](auto glb_tag, auto g_tag) {
-                constexpr bool GLB = decltype(glb_tag)::value;
-                constexpr int g = decltype(g_tag)::value;
-                const TEntry te = s_tab[(b * GT + g) * kTU + lane];
-                const int2 cd = s_cd[(b * GT + g) * kTU + lane];
-                const float z0 = s_Z0[g];
-                const float *e = s_e + g * EP + v0;
-                const float *S;
-                int rs;
-                if constexpr (GLB) {
-                    S = zt + (long long)j * (ZN + 1) * zrs;
-                    rs = zrs;
-                } else {
-                    S = stage0 + b * stage_floats;
-                    rs = CB;
-                }
-                const int dc = cd.y;
-                const int dstep = max(-1, min(1, dc)); // column b = a + dstep on the fast path
-                const bool wide = __any_sync(0xffffffffu, dc > 1 || dc < -1);
+            const int2 cd = make_int2(in.fits ? ia - in.c_lo : ia, dc);
+            const bool wide = __any_sync(0xffffffffu, dc > 1 || dc < -1);
+            if (in.fits) {
+                // address of row k, column a = bits(k + 2^23) * RS4 + base (mod 2^32)
+                const uint32_t base = stage_addr + (uint32_t)b * 4u * (uint32_t)stage_floats + 4u * (uint32_t)cd.x -
+                                      (uint32_t)in.k_lo * RS4 - 0x4B000000u * RS4;
+                const uint32_t dc4 = 4u * (uint32_t)dc;
                 const float kzlo = in.kz_lo, kzhi = in.kz_hi;
-                const int base = cd.x - (GLB ? 0 : in.k_lo) * rs;
+                float prev = 0.f;
+#pragma unroll
+                for (int r4 = 0; r4 <= NR; r4 += 4) {
+                    const float4 e4 = lds_f32x4(e_addr + 4u * r4);
+                    const float ev[4] = {e4.x, e4.y, e4.z, e4.w};
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int r = r4 + q;
+                        if (r > NR) break;
+                        float kz = fmaf(te.T, ev[q], z0);
+                        kz = fminf(fmaxf(kz, kzlo), kzhi);
+                        // 0 <= kz < 2^23: adding 2^23 toward zero leaves floor(kz) in the mantissa
+                        const float rr = __fadd_rz(kz, 8388608.f);
+                        const float fz = kz - (rr - 8388608.f);
+                        const uint32_t pa = __float_as_uint(rr) * RS4 + base, pb = pa + dc4;
+                        const float a0 = lds_f32(pa), a1 = lds_f32(pa + RS4);
+                        const float b0 = lds_f32(pb), b1 = lds_f32(pb + RS4);
+                        const float F = fmaf(te.wb, fmaf(fz, b1 - b0, b0), te.wa * fmaf(fz, a1 - a0, a0));
+                        if (r > 0) acc[r - 1] = fmaf(F - prev, te.scale, acc[r - 1]);
+                        prev = F;
+                    }
+                }
+                if (wide) {
+                    // cells wider than a voxel column: the whole columns strictly
+                    // between a and b, signed like b - a
+                    const int n = dc > 1 ? dc - 1 : (dc < -1 ? -dc - 1 : 0);
+                    const int step4 = dc > 0 ? 4 : -4;
+                    const float sgn_scale = dc > 0 ? te.scale : -te.scale;
+                    float prevx = 0.f;
+#pragma unroll
+                    for (int r = 0; r <= NR; ++r) {
+                        float kz = fmaf(te.T, lds_f32(e_addr + 4u * r), z0);
+                        kz = fminf(fmaxf(kz, kzlo), kzhi);
+                        const float rr = __fadd_rz(kz, 8388608.f);
+                        const float fz = kz - (rr - 8388608.f);
+                        const uint32_t pa = __float_as_uint(rr) * RS4 + base;
+                        float sum = 0.f;
+                        for (int i = 1; i <= n; ++i) {
+                            const uint32_t pc = pa + (uint32_t)(i * step4);
+                            const float c0 = lds_f32(pc), c1 = lds_f32(pc + RS4);
+                            sum += fmaf(fz, c1 - c0, c0);
+                        }
+                        if (r > 0) acc[r - 1] = fmaf(sum - prevx, sgn_scale, acc[r - 1]);
+                        prevx = sum;
+                    }
+                }
+            } else {
+                // block wider than a stage: the column prefixes from global memory
+                const float *S = zt + (long long)j * (ZN + 1) * zrs;
                 float prev = 0.f;
 #pragma unroll
                 for (int r = 0; r <= NR; ++r) {
-                    float kz = fmaf(te.T, e[r], z0);
-                    kz = fminf(fmaxf(kz, kzlo), kzhi);
-                    int k0;
-                    float fz;
-                    if constexpr (GLB) {
-                        k0 = min((int)kz, ZN - 1);
-                        fz = kz - (float)k0;
-                    } else {
-                        // 0 <= kz < 2^23: adding 2^23 toward zero leaves floor(kz) in the mantissa
-                        const float rr = __fadd_rz(kz, 8388608.f);
-                        k0 = __float_as_int(rr) - 0x4B000000;
-                        fz = kz - (rr - 8388608.f);
-                    }
-                    const int ia = base + k0 * rs;
-                    const float a0 = S[ia], a1 = S[ia + rs];
-                    const float b0 = S[ia + dstep], b1 = S[ia + dstep + rs];
-                    const float Za = fmaf(fz, a1 - a0, a0);
-                    const float Zb = fmaf(fz, b1 - b0, b0);
-                    float F = fmaf(te.wb, Zb, te.wa * Za);
+                    float kz = fmaf(te.T, s_e[g * EP + v0l + r], z0);
+                    kz = fminf(fmaxf(kz, 0.f), (float)ZN);
+                    const int k0 = min((int)kz, ZN - 1);
+                    const float fz = kz - (float)k0;
+                    const int ia = cd.x + k0 * zrs;
+                    auto zc = [&](int i) { return fmaf(fz, __ldg(S + i + zrs) - __ldg(S + i), __ldg(S + i)); };
+                    float F = te.wa * zc(ia) + te.wb * zc(ia + dc);
                     if (wide) {
-                        // cells wider than a voxel column: whole columns between a and b
                         const int n = dc > 1 ? dc - 1 : (dc < -1 ? -dc - 1 : 0);
                         const int step = dc > 0 ? 1 : -1;
                         float sum = 0.f;
-                        for (int i = 1; i <= n; ++i) {
-                            const int ic = ia + i * step;
-                            const float c0 = S[ic], c1 = S[ic + rs];
-                            sum += fmaf(fz, c1 - c0, c0);
-                        }
+                        for (int i = 1; i <= n; ++i) sum += zc(ia + i * step);
                         F += dc > 0 ? sum : -sum;
                     }
-                    if (r > 0) acc[g][r - 1] = fmaf(F - prev, te.scale, acc[g][r - 1]);
+                    if (r > 0) acc[r - 1] = fmaf(F - prev, te.scale, acc[r - 1]);
                     prev = F;
                 }
-            };
-            static_for<G>([&](auto g_tag) {
-                constexpr int g = decltype(g_tag)::value;
-                if (s_pos_list[g] < 0) return; // uniform: empty slot of a partial group
-                if (in.fits)
-                    slice_view(std::integral_constant<bool, false>(), g_tag);
-                else
-                    slice_view(std::integral_constant<bool, true>(), g_tag);
-            });
+            }
+            // every shared-memory read of this stage is consumed before the
+            // stage is handed back
+#pragma unroll
+            for (int r = 0; r < NR; ++r) asm volatile("" ::"f"(acc[r]));
             __syncwarp();
             if (lane == 0) mbar_arrive(&s_empty[b]);
         }
 
-        // epilogue
-        const bool owner = lane < nu;
-#pragma unroll
-        for (int g = 0; g < G; ++g) {
-            const int li = s_pos_list[g];
-            if (li < 0 || !owner) continue;
+        // epilogue: NR consecutive detector rows of column u per thread
+        const int li = s_pos_list[g];
+        if (lane < nu) {
             const DevView &V = view_of(g);
             const int u = u0 + lane;
             const double lx = det[t.off_ux + u], ly = det[t.off_uy + u];
             const double cx = lx * V.c - ly * V.s, cy = lx * V.s + ly * V.c;
             const double ex = cx - V.Sx, ey = cy - V.Sy;
             const double ea = V.xdrv ? ex : ey;
+            const double e2 = ex * ex + ey * ey;
 #pragma unroll
             for (int r = 0; r < NR; ++r) {
                 const int v = v0 + r;
                 if (v < DNV) {
                     const double ez = det[t.off_vz + v] + V.zP - V.Sz;
-                    const double L = dx * sqrt(ex * ex + ey * ey + ez * ez) / fabs(ea);
+                    const double L = dx * sqrt(e2 + ez * ez) / fabs(ea);
                     const double de = (det[t.off_bz + v + 1] - det[t.off_bz + v]) / a.dz;
-                    const float val = (float)((double)acc[g][r] * (L / de));
+                    const float val = (float)((double)acc[r] * (L / de));
                     const long long idx = ((long long)li * a.DNU + u) * DNV + v;
                     if (a.epilogue == PROJ_SART_RESIDUAL) {
                         const float mv = a.meas[idx], rsum = a.row_sum[idx];
@@ -415,7 +441,7 @@ __global__ void __launch_bounds__((kTMaxWarps + 1) * 32, 1)
         __syncthreads();
         if (tid == 0) {
             double sum = 0.0;
-            for (int w = 0; w <= NW; ++w) sum += s_red[w];
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) sum += s_red[w];
             atomicAdd(a.resid2, sum);
         }
     }
@@ -423,34 +449,18 @@ __global__ void __launch_bounds__((kTMaxWarps + 1) * 32, 1)
 
 size_t smem_bytes(const ProjTStaging &st)
 {
-    return 128 + 4 * (size_t)st.KR * st.CB * st.nstage + (size_t)st.nstage * st.G * kTU * (sizeof(TEntry) + sizeof(int2)) +
-           sizeof(float) * (size_t)st.G * st.EP;
-}
-
-template <int NR, int G>
-cudaError_t launch_t_g(const ProjArgs &a, const CUtensorMap &tmy, const CUtensorMap &tmx, size_t sm, cudaStream_t s)
-{
-    auto kern = dd3_proj_t_kernel<NR, G>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
-    dim3 grid((a.DNU + kTU - 1) / kTU, a.ngroups);
-    kern<<<grid, (a.t_nw + 1) * 32, sm, s>>>(a, tmy, tmx);
-    return cudaGetLastError();
+    return 128 + 4 * (size_t)st.KR * st.CB * st.nstage + sizeof(float) * (size_t)st.G * st.EP;
 }
 
 template <int NR>
-cudaError_t launch_t_nr(const ProjArgs &a, const CUtensorMap &tmy, const CUtensorMap &tmx, size_t sm,
-                        cudaStream_t s)
+cudaError_t launch_t_nr(const ProjArgs &a, const CUtensorMap &tmy, const CUtensorMap &tmx, size_t sm, cudaStream_t s)
 {
-    switch (a.G) {
-    case 1: return launch_t_g<NR, 1>(a, tmy, tmx, sm, s);
-    case 2: return launch_t_g<NR, 2>(a, tmy, tmx, sm, s);
-    case 4: return launch_t_g<NR, 4>(a, tmy, tmx, sm, s);
-    case 8:
-        if constexpr (NR <= 8) return launch_t_g<NR, 8>(a, tmy, tmx, sm, s);
-        return cudaErrorInvalidValue;
-    default: return cudaErrorInvalidValue;
-    }
+    auto kern = dd3_proj_t_kernel<NR>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    dim3 grid((a.DNU + kTU - 1) / kTU, a.ngroups, a.t_zs);
+    kern<<<grid, (a.G * a.t_rb + 1) * 32, sm, s>>>(a, tmy, tmx);
+    return cudaGetLastError();
 }
 
 // b-index span (in columns, margins included) of the union of the rays of
@@ -479,9 +489,8 @@ int t_span(const HostGeometry &g, const std::vector<const DevView *> &vs, int u0
     return c_hi - c_lo + 1;
 }
 
-// Largest column span of any group of G views (by axis, adjacent angles)
-// over all tiles and slices; the span is convex in the slice index, so the
-// end slices bound it.
+// Largest column span of any group (view indices) over all tiles and
+// slices; the span is convex in the slice index, so the end slices bound it.
 int t_need(const HostGeometry &g, const std::vector<std::vector<int>> &groups)
 {
     int need = 4;
@@ -497,10 +506,8 @@ int t_need(const HostGeometry &g, const std::vector<std::vector<int>> &groups)
     return need;
 }
 
-// Views of `list` (view indices) grouped G at a time: by driving axis, then
-// within runs of angularly adjacent views (a view's axis covers two opposite
-// quadrant pairs, so the sorted angles of one axis have gaps); returns list
-// positions.
+// Views of `list` (view indices) grouped G at a time within runs of
+// angularly adjacent views of one driving axis; returns list positions.
 std::vector<std::vector<int>> t_groups(const HostGeometry &g, const std::vector<int> &list, int G)
 {
     std::vector<std::vector<int>> out;
@@ -511,6 +518,59 @@ std::vector<std::vector<int>> t_groups(const HostGeometry &g, const std::vector<
             out.push_back(grp);
         }
     return out;
+}
+
+std::vector<std::vector<int>> as_views(std::vector<std::vector<int>> groups, const std::vector<int> &list)
+{
+    for (auto &grp : groups)
+        for (int &p : grp) p = list[p];
+    return groups;
+}
+
+// Rows of z-prefix a CTA stages for one slice (+3: the margins and the
+// interpolation neighbour of the kernel's range), the largest over groups,
+// tiles, row blocks of `rows` detector rows and (sampled) slices.  kz is
+// affine in the magnification T for a fixed boundary, so the columns at the
+// ends and the middle of a tile bound it for flat and curved detectors.
+int t_zrows(const HostGeometry &g, const std::vector<std::vector<int>> &groups, int rows, int zs)
+{
+    int need = 4;
+    for (const auto &grp : groups) {
+        const DevView &V0 = g.views[grp[0]];
+        const int jstep = std::max(1, V0.na / 64);
+        for (int u0 = 0; u0 < g.DNU; u0 += kTU) {
+            const int nu = std::min(kTU, g.DNU - u0);
+            const int us[3] = {u0, u0 + nu / 2, u0 + nu - 1};
+            for (int zb = 0; zb < zs; ++zb) {
+                const int w0 = zb * rows, w1 = std::min(g.DNV, w0 + rows);
+                for (int j = 0; j < V0.na; j += (j + jstep < V0.na || j == V0.na - 1) ? jstep : V0.na - 1 - j) {
+                    double lo = 1e300, hi = -1e300;
+                    for (int v : grp) {
+                        const DevView &V = g.views[v];
+                        const double z0 = (V.Sz - g.z_lo) / g.dz;
+                        double emin = 1e300, emax = -1e300;
+                        for (int w = w0; w <= w1; ++w) {
+                            const double e = (g.bz[w] + V.zP - V.Sz) / g.dz;
+                            emin = std::min(emin, e);
+                            emax = std::max(emax, e);
+                        }
+                        for (int u : us) {
+                            const double ca = V.xdrv ? (g.ux[u] * V.c - g.uy[u] * V.s) : (g.ux[u] * V.s + g.uy[u] * V.c);
+                            const double T = (V.a0 - V.Sa + j * g.dx) / (ca - V.Sa);
+                            for (double e : {emin, emax}) {
+                                const double kz = std::min(std::max(z0 + T * e, 0.0), (double)g.ZN);
+                                lo = std::min(lo, kz);
+                                hi = std::max(hi, kz);
+                            }
+                        }
+                    }
+                    need = std::max(need, (int)hi - std::max((int)lo - 1, 0) + 3);
+                    if (j == V0.na - 1) break;
+                }
+            }
+        }
+    }
+    return std::min(need, g.ZN + 2);
 }
 
 int env_int(const char *name, int dflt)
@@ -525,26 +585,18 @@ ProjTStaging proj_t_staging(const HostGeometry &g)
 {
     ProjTStaging st;
     st.ok = false;
-    if (g.DNV > kTMaxWarps * 16) return st;
-    st.NR = 1;
-    while ((g.DNV + st.NR - 1) / st.NR > kTMaxWarps) st.NR *= 2;
-    st.NW = (g.DNV + st.NR - 1) / st.NR;
-    st.EP = ((st.NW * st.NR + 1) + 3) & ~3;
-    const int nbox = (g.ZN + 2 + 255) / 256;
-    const int kb0 = (g.ZN + 2 + nbox - 1) / nbox;
-    // CTLAB_PROJT_GMAX caps the views per CTA (1, 2, 4, 8), CTLAB_PROJT_NSTAGE
-    // fixes the depth (2..4), CTLAB_PROJT_CBMAX caps the staged columns
-    const int gmax = std::min(env_int("CTLAB_PROJT_GMAX", kTMaxG), st.NR <= 8 ? 8 : 4);
+    // CTLAB_PROJT_GMAX caps the views per CTA (1..16), CTLAB_PROJT_ZS fixes
+    // the row split (1, 2, 4), CTLAB_PROJT_NSTAGE the stage depth (2..4),
+    // CTLAB_PROJT_CBMAX caps the staged columns
+    const int gmax = std::max(1, std::min(env_int("CTLAB_PROJT_GMAX", 8), kTMaxG));
+    const int want_zs = env_int("CTLAB_PROJT_ZS", 0);
     const int want_stage = env_int("CTLAB_PROJT_NSTAGE", 0);
     const int cbmax = std::min(env_int("CTLAB_PROJT_CBMAX", 256), 256);
     std::vector<int> all(g.PN);
     for (int i = 0; i < g.PN; ++i) all[i] = i;
-    for (int G = 8; G >= 1; G /= 2) {
+    for (int G = kTMaxG; G >= 1; G /= 2) {
         if (G > gmax) continue;
-        std::vector<std::vector<int>> groups = t_groups(g, all, G);
-        for (auto &grp : groups)
-            for (int &p : grp) p = all[p];
-        int CB = (t_need(g, groups) + 3) & ~3;
+        int CB = (t_need(g, as_views(t_groups(g, all, G), all)) + 3) & ~3;
         // a row stride of 16 (mod 32) floats keeps lanes that read neighbouring
         // rows off each other's banks; take it when it costs little
         const int cb16 = CB + ((16 - CB % 32) + 32) % 32;
@@ -553,40 +605,55 @@ ProjTStaging proj_t_staging(const HostGeometry &g)
             if (G > 1) continue;
             CB = cbmax & ~3; // G = 1: wider slices read global memory
         }
-        // 128-byte aligned TMA destinations: KB * CB * 4 a multiple of 128
-        int KB = kb0;
-        while ((KB * CB) % 32) ++KB;
-        if (KB > 256) continue;
-        const int KR = nbox * KB;
-        for (int ns = kTMaxStage; ns >= 2; --ns) {
-            if (want_stage >= 2 && want_stage <= kTMaxStage && ns != want_stage) continue;
-            ProjTStaging c = st;
-            c.G = G;
-            c.CB = CB;
-            c.KB = KB;
-            c.KR = KR;
-            c.nstage = ns;
-            c.smem = smem_bytes(c);
-            // prefer two CTAs per SM (depth >= 2 within half the shared memory)
-            const bool two = c.smem + kTStatic <= kTSmemLimit / 2;
-            if (c.smem + kTStatic > kTSmemLimit) continue;
-            if (!two && ns > 2 && want_stage == 0) {
-                // a deep stage that forces one CTA per SM: try fewer stages first
-                ProjTStaging c2 = c;
-                c2.nstage = 2;
-                c2.smem = smem_bytes(c2);
-                if (c2.smem + kTStatic <= kTSmemLimit / 2) continue;
+        for (int ZS : {1, 2, 4}) {
+            if (want_zs && ZS != want_zs) continue;
+            if (!want_zs && ZS > 1 && g.DNV < 16 * ZS) continue;
+            const int rows = (g.DNV + ZS - 1) / ZS; // detector rows per CTA
+            // rows per consumer warp: 4..32, the row blocks of G views filling
+            // at most 16 warps
+            int NR = 4;
+            while ((rows + NR - 1) / NR * G > kTMaxCWarps && NR < 32) NR *= 2;
+            const int RB = (rows + NR - 1) / NR;
+            if (RB * G > kTMaxCWarps) continue;
+            const int zs = (g.DNV + RB * NR - 1) / (RB * NR); // CTAs over the rows (no empty one)
+            // z rows a CTA stages per slice: the clamped kz range of its
+            // detector rows over the group's views and the tile's columns
+            const int zrows = t_zrows(g, as_views(t_groups(g, all, G), all), RB * NR, zs);
+            const int nbox = (zrows + 255) / 256;
+            int KB = (zrows + nbox - 1) / nbox;
+            // 128-byte aligned TMA destinations: KB * CB * 4 a multiple of 128
+            while ((KB * CB) % 32) ++KB;
+            if (KB > 256) continue;
+            for (int ns = kTMaxStage; ns >= 2; --ns) {
+                if (want_stage >= 2 && want_stage <= kTMaxStage && ns != want_stage) continue;
+                ProjTStaging c;
+                c.G = G;
+                c.NR = NR;
+                c.RB = RB;
+                c.ZS = zs;
+                c.CB = CB;
+                c.KB = KB;
+                c.KR = nbox * KB;
+                c.nstage = ns;
+                c.EP = RB * NR + 4;
+                c.smem = smem_bytes(c);
+                if (c.smem + kTStatic > kTSmemLimit) continue;
+                c.ok = true;
+                return c;
             }
-            c.ok = true;
-            return c;
         }
     }
     // nothing stages: every slice reads global memory
     st.G = 1;
+    st.ZS = 1;
+    st.NR = 4;
+    while ((g.DNV + st.NR - 1) / st.NR > kTMaxCWarps) st.NR *= 2;
+    st.RB = (g.DNV + st.NR - 1) / st.NR;
     st.CB = 0;
     st.KB = 0;
     st.KR = 0;
     st.nstage = 2;
+    st.EP = st.RB * st.NR + 4;
     st.smem = smem_bytes(st);
     st.ok = true;
     return st;
@@ -597,12 +664,7 @@ ProjGroups proj_t_make_groups(const HostGeometry &g, const std::vector<int> &lis
     ProjGroups out;
     for (int G = st.G; G >= 1; G /= 2) {
         std::vector<std::vector<int>> groups = t_groups(g, list, G);
-        if (G > 1) {
-            std::vector<std::vector<int>> vgroups = groups;
-            for (auto &grp : vgroups)
-                for (int &p : grp) p = list[p];
-            if (t_need(g, vgroups) > st.CB) continue;
-        }
+        if (G > 1 && t_need(g, as_views(groups, list)) > st.CB) continue;
         out.G = G;
         out.table.clear();
         for (auto &grp : groups)
@@ -617,15 +679,14 @@ cudaError_t launch_proj_t(const ProjArgs &a, const ProjTStaging &st, const CUten
                           cudaStream_t s, int *launches)
 {
     if (a.n <= 0 || a.ngroups <= 0) return cudaSuccess;
-    if (a.ngroups > 65535 || a.G > st.G) return cudaErrorInvalidConfiguration;
+    if (a.ngroups > 65535 || a.G > st.G || a.G * a.t_rb > kTMaxCWarps) return cudaErrorInvalidConfiguration;
     if (launches) ++*launches;
     const size_t sm = smem_bytes(st);
     switch (st.NR) {
-    case 1: return launch_t_nr<1>(a, tmy, tmx, sm, s);
-    case 2: return launch_t_nr<2>(a, tmy, tmx, sm, s);
     case 4: return launch_t_nr<4>(a, tmy, tmx, sm, s);
     case 8: return launch_t_nr<8>(a, tmy, tmx, sm, s);
     case 16: return launch_t_nr<16>(a, tmy, tmx, sm, s);
+    case 32: return launch_t_nr<32>(a, tmy, tmx, sm, s);
     default: return cudaErrorInvalidValue;
     }
 }
