@@ -1,0 +1,504 @@
+// Branchless DD cone-beam backprojection on projection v-prefixes (sat mode
+// CTLAB_SAT_ZPREFIX): the voxel-driven gather of back.cu with the 2-D FP64
+// projection SAT replaced by per-detector-column prefixes along v,
+//     P[l][u][v'] = sum_{v<v'} W(l, u, v),  W = prj * slab length,
+// accumulated in FP64 and stored in FP32 (the column differences of the 2-D
+// SAT, which the FP64 path also rounds to FP32 before use).
+//
+// One CTA (512 threads) owns an 8 x 8 brick of voxel columns and a z range of
+// 8*KSEG voxels and loops over the views.  Per view:
+//   geometry   the brick's voxel boundaries across the view's driving axis
+//              (8 rows of 9 points) mapped through the source onto the flat
+//              detector (FP64); each column's centre ray gives the affine
+//              z -> v map, kept normalised by DNV;
+//   staging    the rows [u_lo, u_hi] of the view's P that the brick's
+//              footprint covers: one 1-D bulk copy (TMA), double buffered
+//              two views ahead and completed on an mbarrier;
+//   phase A    per column and detector row boundary v', the strip integral
+//              between the column's two u boundaries,
+//                 E_c(v') = sg * [ sum of P over whole cells + f_b P_b - f_a P_a ],
+//              sg orienting it like the voxel's z axis (FP32), stored with its
+//              forward difference as (E, dE) pairs; 8 threads per column each
+//              run a contiguous stretch of rows with a warp-uniform trip count;
+//   phase B    each voxel boundary k samples E_c linearly at
+//              v = DNV * sat(V0 + V1 k) with one 64-bit shared load and the
+//              voxel accumulates E_c(v_{k+1}) - E_c(v_k): one saturating FMA
+//              clamps, the round-toward-zero FMA with 2^23 gives floor(v)
+//              biased for the shared-memory address -- no float/int
+//              conversions.
+// E is double buffered, so one barrier per view separates A(l) from B(l) and
+// the issue of view l+2's copy.  Views whose footprint exceeds a stage read P
+// from global memory.  Epilogue: in-plane mask and optionally the OS-SART
+// update x = (x + lambda * acc/colSum) * mask.
+#include <cmath>
+#include <type_traits>
+#include <utility>
+
+#include "internal.h"
+#include "tma.cuh"
+
+namespace ctlab {
+
+namespace {
+
+constexpr int kB = 8;                 // brick edge (voxel columns)
+constexpr int kCols = kB * kB;        // 64 columns per CTA
+constexpr int kZS = 8;                // z segments per column
+constexpr int kThreads = kCols * kZS; // 512
+constexpr size_t kSmemPerCta = 200 * 1024; // one CTA per SM
+constexpr size_t kStaticSmem = 6 * 1024;
+constexpr int kGeo = 4;               // geometry slots (views l .. l+3)
+
+__device__ __forceinline__ float lds_f32(uint32_t addr)
+{
+    float v;
+    asm("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr));
+    return v;
+}
+
+__device__ __forceinline__ float2 lds_f32x2(uint32_t addr)
+{
+    float2 v;
+    asm("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr));
+    return v;
+}
+
+template <int OFF>
+__device__ __forceinline__ float lds_f32_at(uint32_t addr)
+{
+    float v;
+    asm("ld.shared.f32 %0, [%1+%2];" : "=f"(v) : "r"(addr), "n"(OFF));
+    return v;
+}
+template <int OFF>
+__device__ __forceinline__ void sts_f32x2_at(uint32_t addr, float x, float y)
+{
+    asm volatile("st.shared.v2.f32 [%0+%1], {%2, %3};" ::"r"(addr), "n"(OFF), "f"(x), "f"(y) : "memory");
+}
+template <int I, int N, class F>
+__device__ __forceinline__ void unroll_for(F &&f)
+{
+    if constexpr (I < N) {
+        f(std::integral_constant<int, I>());
+        unroll_for<I + 1, N>(f);
+    }
+}
+
+// Phase A run of one thread: E at rows i0 .. i0+VPT of one column from the
+// staged P rows pa, pb (and NX whole cells pm[] between them), stored as VPT
+// (E, dE) pairs at eout.  Every address carries i0; offsets are immediates.
+template <int VPT, int NX>
+__device__ __forceinline__ void phase_a_run(uint32_t pa, uint32_t pb, const uint32_t (&pm)[3], const float (&wmv)[3],
+                                            float wa, float wb, uint32_t eout)
+{
+    float e_prev = 0.f;
+    unroll_for<0, VPT + 1>([&](auto jt) {
+        constexpr int j = decltype(jt)::value;
+        float e = fmaf(wb, lds_f32_at<4 * j>(pb), wa * lds_f32_at<4 * j>(pa));
+        unroll_for<0, NX>([&](auto mt) {
+            constexpr int m = decltype(mt)::value;
+            e = fmaf(wmv[m], lds_f32_at<4 * j>(pm[m]), e);
+        });
+        if constexpr (j > 0) sts_f32x2_at<8 * (j - 1)>(eout, e_prev, e - e_prev);
+        e_prev = e;
+    });
+}
+
+__device__ __forceinline__ double cross2(double ax, double ay, double bx, double by)
+{
+    return ax * by - ay * bx;
+}
+
+__device__ __forceinline__ double u_of(const DevView &V, double px, double py)
+{
+    const double dpx = px - V.Sx, dpy = py - V.Sy;
+    return cross2(V.Sx - V.B0x, V.Sy - V.B0y, dpx, dpy) / cross2(V.Ex, V.Ey, dpx, dpy);
+}
+
+template <int KSEG, int VPT>
+__global__ void __launch_bounds__(kThreads, 1) dd3_back_t_kernel(BackArgs a, int es2, int rmax)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int vp = a.vp; // P row pitch (floats, multiple of 4)
+    float2 *E2 = reinterpret_cast<float2 *>(smem);                      // [2][kCols][es2] (E, dE)
+    float *pbuf = reinterpret_cast<float *>(E2 + 2 * (size_t)kCols * es2); // [2][rmax][vp]
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ int s_ulo[2], s_rows[2];
+    __shared__ double s_u[kGeo][kB][kB + 1];
+    __shared__ float s_V0[kGeo][kCols], s_V1[kGeo][kCols];
+    __shared__ int s_xdrv[kGeo];
+
+    const int tid = threadIdx.x;
+    const int bx0 = blockIdx.x * kB, by0 = blockIdx.y * kB;
+    const int col = tid & (kCols - 1), zs = tid / kCols;
+    const int cx = col & (kB - 1), cy = col / kB;
+    const int x = bx0 + cx, y = by0 + cy;
+    const int k0 = blockIdx.z * (kZS * KSEG) + zs * KSEG;
+    const int DNU = a.DNU, DNV = a.DNV, ZN = a.ZN, n = a.n;
+    const double dx = a.dx;
+    const double x_lo = a.x_c0 - 0.5 * dx, y_lo = a.y_c0 - 0.5 * dx;
+    const DetTable t = det_table_layout(DNU, DNV);
+    const double zb0_local = a.det[t.off_bz];
+    const bool in_vol = (x < a.XN) && (y < a.YN);
+    const float *Pall = a.pv;
+    const long long pstride = (long long)DNU * vp;
+    const float DNVf = (float)DNV;
+    const double inv_n = 1.0 / (a.dzb * DNV), dz_n = a.dz * inv_n; // detector rows, normalised by DNV
+
+    if (tid == 0) {
+        mbar_init(&s_bar[0], 1);
+        mbar_init(&s_bar[1], 1);
+        mbar_fence_init();
+    }
+
+    // per-view geometry of view list entry l into slot l % kGeo: the brick's
+    // voxel boundaries across the driving axis on the detector (warps 0-2)
+    // and each column's z -> v map (warps 4-5)
+    auto geometry = [&](int l) {
+        if (l >= n) return;
+        const DevView &V = a.views[a.view_list[l]];
+        const int sl = l % kGeo;
+        if (tid < kB * (kB + 1)) {
+            const int r = tid / (kB + 1), q = tid - r * (kB + 1);
+            double px, py;
+            if (!V.xdrv) {
+                px = x_lo + (double)(bx0 + q) * dx;
+                py = a.y_c0 + (double)(by0 + r) * dx;
+            } else {
+                px = a.x_c0 + (double)(bx0 + r) * dx;
+                py = y_lo + (double)(by0 + q) * dx;
+            }
+            s_u[sl][r][q] = u_of(V, px, py);
+            if (tid == 0) s_xdrv[sl] = V.xdrv;
+        } else if (tid >= 128 && tid < 128 + kCols) {
+            const int c = tid - 128;
+            const double pcx = a.x_c0 + (double)(bx0 + (c & (kB - 1))) * dx;
+            const double pcy = a.y_c0 + (double)(by0 + c / kB) * dx;
+            const double tc = cross2(V.B0x - V.Sx, V.B0y - V.Sy, V.Ex, V.Ey) /
+                              cross2(pcx - V.Sx, pcy - V.Sy, V.Ex, V.Ey);
+            const double zb0 = zb0_local + V.zP;
+            // z boundary k' -> detector row coordinate v = V0 + V1 k', stored / DNV
+            s_V1[sl][c] = (float)(tc * dz_n);
+            s_V0[sl][c] = (float)((V.Sz + tc * (a.z_lo - V.Sz) - zb0) * inv_n);
+        }
+    };
+    // staging of list entry l into buffer l & 1 (thread 0): the rows of P the
+    // brick's footprint covers, from the corner boundaries of its geometry
+    auto issue = [&](int l) {
+        if (tid != 0 || l >= n) return;
+        const int b = l & 1, sl = l % kGeo;
+        const double u0 = s_u[sl][0][0], u1 = s_u[sl][0][kB], u2 = s_u[sl][kB - 1][0], u3 = s_u[sl][kB - 1][kB];
+        const double umin = fmin(fmax(fmin(fmin(u0, u1), fmin(u2, u3)), 0.0), (double)(DNU - 1));
+        const double umax = fmin(fmax(fmax(fmax(u0, u1), fmax(u2, u3)), 0.0), (double)(DNU - 1));
+        // one row of margin each side: interior boundaries may round past
+        // the corners' range by an ulp
+        const int lo = max((int)umin - 1, 0), rows = min((int)umax + 2, DNU - 1) - lo + 1;
+        const bool fits = rows <= rmax;
+        s_ulo[b] = lo;
+        s_rows[b] = fits ? rows : 0;
+        mbar_arrive_expect_tx(&s_bar[b], fits ? (uint32_t)(4 * rows * vp) : 0u);
+        if (fits)
+            bulk_copy_g2s(pbuf + (size_t)b * rmax * vp, Pall + l * pstride + (long long)lo * vp,
+                          (uint32_t)(4 * rows * vp), &s_bar[b]);
+    };
+
+    geometry(0);
+    geometry(1);
+    geometry(2);
+    __syncthreads(); // barrier init and geometry visible
+    issue(0);
+    issue(1);
+    __syncthreads();
+
+    float acc[KSEG];
+#pragma unroll
+    for (int r = 0; r < KSEG; ++r) acc[r] = 0.f;
+    bool timed_out = false;
+    const uint32_t E2_addr = smem_addr(E2);
+    // phase A: kAPh threads per column, each a run of vpt consecutive rows
+    constexpr int kAPh = kThreads / kCols;
+    const int ac = tid / kAPh, aph = tid % kAPh;
+    const int acx = ac & (kB - 1), acy = ac / kB;
+    const int i0 = aph * VPT; // this thread's entries i0 .. i0+VPT-1 (kAPh*VPT > DNV)
+
+    for (int li = 0; li < n; ++li) {
+        const int b = li & 1, ls = li % kGeo;
+        const int ulo = s_ulo[b], rows = s_rows[b];
+        if (!mbar_wait(&s_bar[b], (uint32_t)((li >> 1) & 1))) timed_out = true;
+        const int xdrv = s_xdrv[ls];
+        float2 *E = E2 + (size_t)b * kCols * es2; // double buffered: B(li) overlaps A(li+1)
+
+        // ---- A: (E_c(i), E_c(i+1) - E_c(i)) for i in [0, DNV], E_c(DNV+1) = E_c(DNV) ----
+        if (!timed_out) {
+            const double ua = xdrv ? s_u[ls][acx][acy] : s_u[ls][acy][acx];
+            const double ub = xdrv ? s_u[ls][acx][acy + 1] : s_u[ls][acy][acx + 1];
+            const double uca = fmin(fmax(ua, 0.0), (double)DNU), ucb = fmin(fmax(ub, 0.0), (double)DNU);
+            const int ia = min((int)uca, DNU - 1), ib = min((int)ucb, DNU - 1);
+            const float fa = (float)(uca - ia), fb = (float)(ucb - ib);
+            const float sg = ((ub - ua > 0) ? 1.f : -1.f) * ((s_V1[ls][ac] > 0.f) ? 1.f : -1.f);
+            const int dc = ib - ia;
+            float wa, wb;
+            if (dc == 0) {
+                wa = fb - fa;
+                wb = 0.f;
+            } else if (dc > 0) {
+                wa = 1.f - fa;
+                wb = fb;
+            } else {
+                wa = -fa;
+                wb = fb - 1.f;
+            }
+            wa *= sg;
+            wb *= sg;
+            // whole cells strictly between a and b; the warp runs its widest
+            // column's count, the others with weight 0
+            const int nm = max(abs(dc) - 1, 0), first = min(ia, ib) + 1;
+            const int nmax = __reduce_max_sync(0xffffffffu, nm);
+            const float wm = dc > 0 ? sg : -sg;
+            if (rows > 0) {
+                // staged rows: 32-bit shared addresses, row u at pbase + (u - ulo) * vp4;
+                // the pitch covers i0+VPT, and entries past DNV repeat the total
+                const uint32_t vp4 = 4u * (uint32_t)vp;
+                const uint32_t pbase = smem_addr(pbuf + (size_t)b * rmax * vp) + 4u * (uint32_t)i0;
+                auto row = [&](int u) { return pbase + (uint32_t)min(max(u - ulo, 0), rows - 1) * vp4; };
+                const uint32_t pa = row(ia), pb = row(ib);
+                const uint32_t eout = E2_addr + 8u * (uint32_t)((b * kCols + ac) * es2 + i0);
+                uint32_t pm[3];
+                float wmv[3];
+#pragma unroll
+                for (int m = 0; m < 3; ++m) {
+                    pm[m] = row(min(first + m, max(ia, ib)));
+                    wmv[m] = m < nm ? wm : 0.f;
+                }
+                switch (nmax) {
+                case 0: phase_a_run<VPT, 0>(pa, pb, pm, wmv, wa, wb, eout); break;
+                case 1: phase_a_run<VPT, 1>(pa, pb, pm, wmv, wa, wb, eout); break;
+                case 2: phase_a_run<VPT, 2>(pa, pb, pm, wmv, wa, wb, eout); break;
+                case 3: phase_a_run<VPT, 3>(pa, pb, pm, wmv, wa, wb, eout); break;
+                default: {
+                    // cells much wider than voxels: the whole cells by a loop
+                    float2 *Ec = E + ac * es2;
+                    float e = 0.f;
+                    for (int j = 0; j <= VPT; ++j) {
+                        const uint32_t o = 4u * (uint32_t)j;
+                        float en = fmaf(wb, lds_f32(pb + o), wa * lds_f32(pa + o));
+                        for (int m = 0; m < nm; ++m) en = fmaf(wm, lds_f32(row(first + m) + o), en);
+                        if (j > 0) Ec[i0 + j - 1] = make_float2(e, en - e);
+                        e = en;
+                    }
+                }
+                }
+            } else {
+                // footprint wider than a stage: P from global memory
+                const float *Pg = Pall + li * pstride;
+                float2 *Ec = E + ac * es2;
+                auto eval = [&](int i) {
+                    float e = fmaf(wb, __ldg(Pg + (size_t)ib * vp + i), wa * __ldg(Pg + (size_t)ia * vp + i));
+                    for (int m = 0; m < nm; ++m) e = fmaf(wm, __ldg(Pg + (size_t)(first + m) * vp + i), e);
+                    return e;
+                };
+                float e = eval(i0);
+                for (int j = 0; j < VPT; ++j) {
+                    const float en = eval(i0 + j + 1);
+                    Ec[i0 + j] = make_float2(e, en - e);
+                    e = en;
+                }
+            }
+        }
+        __syncthreads();
+
+        // ---- stage view li+2 into the buffer just consumed; geometry of li+3 ----
+        issue(li + 2);
+        geometry(li + 3);
+
+        // ---- phase B: voxels ----
+        if (in_vol && !timed_out) {
+            const float V0 = s_V0[ls][col], V1 = s_V1[ls][col];
+            // address of (E, dE)_c[i] = bits(i + 2^23) * 8 + base (mod 2^32)
+            const uint32_t base = E2_addr + 8u * (uint32_t)(b * kCols * es2 + col * es2) - 8u * 0x4B000000u;
+            const float vb0 = fmaf(V1, (float)k0, V0);
+            float prev = 0.f;
+#pragma unroll
+            for (int r = 0; r <= KSEG; ++r) {
+                const float vn = __saturatef(fmaf(V1, (float)r, vb0));
+                const float rr = __fmaf_rz(vn, DNVf, 8388608.f); // 2^23 + floor(DNV vn)
+                const float fz = fmaf(vn, DNVf, 8388608.f - rr);
+                const float2 ed = lds_f32x2(__float_as_uint(rr) * 8u + base);
+                const float ev = fmaf(fz, ed.y, ed.x);
+                if (r > 0) acc[r - 1] += ev - prev;
+                prev = ev;
+            }
+        }
+    }
+    if (timed_out && a.err) atomicExch(a.err, CTLAB_ERR_TIMEOUT);
+
+    if (!in_vol) return;
+    const long long colidx = (long long)y * a.XN + x;
+    const float m = a.mask ? (a.mask[colidx] ? 1.f : 0.f) : 1.f;
+    float *o = a.out + colidx * ZN;
+#pragma unroll
+    for (int r = 0; r < KSEG; ++r) {
+        const int k = k0 + r;
+        if (k < ZN) {
+            if (a.epilogue == BACK_SART_UPDATE) {
+                const float cs = a.col_sum[colidx * ZN + k];
+                const float upd = (cs > 1.0e-7f) ? acc[r] / cs : 0.f;
+                float v = (o[k] + a.lambda * upd) * m;
+                if (a.clamp) v = fminf(fmaxf(v, a.min_v), a.max_v);
+                o[k] = v;
+            } else {
+                o[k] = acc[r] * m;
+            }
+        }
+    }
+}
+
+// Projection v-prefixes: one warp per detector column (view l, cell u) scans
+// the weighted column in FP64 32 rows at a time with shuffles and a carried
+// total; out[l][u][v'] for v' in [0, DNV], entries past DNV repeat the total.
+__global__ void __launch_bounds__(256) pv_kernel(PrjIn in, long long ncols, int DNU, int DNV, float *__restrict__ out,
+                                                 int vp)
+{
+    const int lane = threadIdx.x & 31;
+    const long long cidx = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (cidx >= ncols) return;
+    const int l = (int)(cidx / DNU), u = (int)(cidx - (long long)l * DNU);
+    float *o = out + cidx * vp;
+    double carry = 0.0;
+    if (lane == 0) o[0] = 0.f;
+    for (int v0 = 0; v0 < DNV; v0 += 32) {
+        const int v = v0 + lane;
+        double s = v < DNV ? (double)in(l, u, v) : 0.0;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const double y = __shfl_up_sync(0xffffffffu, s, d);
+            if (lane >= d) s += y;
+        }
+        s += carry;
+        if (v < DNV) o[v + 1] = (float)s;
+        carry = __shfl_sync(0xffffffffu, s, 31);
+    }
+    for (int v = DNV + 1 + lane; v < vp; v += 32) o[v] = (float)carry;
+}
+
+// Rows of E per phase-A thread: kAPh * VPT > DNV, from a few compiled sizes.
+int vpt_of(int DNV)
+{
+    const int need = (DNV + 1 + kThreads / kCols - 1) / (kThreads / kCols);
+    for (int v : {2, 5, 9, 17, 33})
+        if (v >= need) return v;
+    return 0;
+}
+int e_pitch(int DNV) { return ((kThreads / kCols) * vpt_of(DNV)) | 1; }
+
+size_t dyn_smem(int rmax, int vp, int es2)
+{
+    return 4 * 2 * (size_t)rmax * vp + sizeof(float2) * 2 * (size_t)kCols * es2;
+}
+
+template <int KSEG, int VPT>
+cudaError_t launch_k(const BackArgs &a, cudaStream_t s)
+{
+    const int es2 = e_pitch(a.DNV); // (E, dE) pairs per column, odd pitch
+    const size_t sm = dyn_smem(a.rmax, a.vp, es2);
+    auto kern = dd3_back_t_kernel<KSEG, VPT>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    dim3 grid((a.XN + kB - 1) / kB, (a.YN + kB - 1) / kB, (a.ZN + kZS * KSEG - 1) / (kZS * KSEG));
+    kern<<<grid, kThreads, sm, s>>>(a, es2, a.rmax);
+    return cudaGetLastError();
+}
+
+template <int VPT>
+cudaError_t launch_z(const BackArgs &a, cudaStream_t s)
+{
+    if (a.ZN <= kZS * 4) return launch_k<4, VPT>(a, s);
+    if (a.ZN <= kZS * 8) return launch_k<8, VPT>(a, s);
+    if (a.ZN <= kZS * 16) return launch_k<16, VPT>(a, s);
+    return launch_k<32, VPT>(a, s);
+}
+
+} // namespace
+
+bool back_t_supported(int DNV)
+{
+    if (vpt_of(DNV) == 0) return false;
+    return dyn_smem(2, back_t_pitch(DNV), e_pitch(DNV)) + kStaticSmem <= 227 * 1024;
+}
+
+// P row pitch: DNV+1 prefixes, then the total repeated up to the last row a
+// phase-A run reads (kAPh * VPT), rounded to 16 bytes
+int back_t_pitch(int DNV)
+{
+    return (std::max(DNV + 2, (kThreads / kCols) * vpt_of(DNV) + 1) + 3) & ~3;
+}
+
+// Staged P rows: the widest u footprint of any brick on the volume's outer
+// ring of bricks (nearest the source in some view), +2, capped so two CTAs
+// fit an SM (at least 2; wider footprints read global memory).
+int back_t_staging_rows(const HostGeometry &g)
+{
+    const int vp = back_t_pitch(g.DNV);
+    const int es2 = e_pitch(g.DNV);
+    const double x_c0 = g.cx - 0.5 * (g.XN - 1) * g.dx, y_c0 = g.cy - 0.5 * (g.YN - 1) * g.dx;
+    const double x_lo = x_c0 - 0.5 * g.dx, y_lo = y_c0 - 0.5 * g.dx;
+    const int nbx = (g.XN + kB - 1) / kB, nby = (g.YN + kB - 1) / kB;
+    int need = 2;
+    auto uof = [](const DevView &V, double px, double py) {
+        const double dpx = px - V.Sx, dpy = py - V.Sy;
+        const double num = (V.Sx - V.B0x) * dpy - (V.Sy - V.B0y) * dpx;
+        return num / (V.Ex * dpy - V.Ey * dpx);
+    };
+    for (const DevView &V : g.views) {
+        for (int by = 0; by < nby; ++by) {
+            for (int bx = 0; bx < nbx; ++bx) {
+                if (by != 0 && by != nby - 1 && bx != 0 && bx != nbx - 1) continue;
+                const int bx0 = bx * kB, by0 = by * kB;
+                double px0, px1, py0, py1;
+                if (!V.xdrv) {
+                    px0 = x_lo + bx0 * g.dx; px1 = x_lo + (bx0 + kB) * g.dx;
+                    py0 = y_c0 + by0 * g.dx; py1 = y_c0 + (by0 + kB - 1) * g.dx;
+                } else {
+                    px0 = x_c0 + bx0 * g.dx; px1 = x_c0 + (bx0 + kB - 1) * g.dx;
+                    py0 = y_lo + by0 * g.dx; py1 = y_lo + (by0 + kB) * g.dx;
+                }
+                const double u0 = uof(V, px0, py0), u1 = uof(V, px1, py0), u2 = uof(V, px0, py1),
+                             u3 = uof(V, px1, py1);
+                const double umin = std::min(std::max(std::min(std::min(u0, u1), std::min(u2, u3)), 0.0),
+                                             (double)(g.DNU - 1));
+                const double umax = std::min(std::max(std::max(std::max(u0, u1), std::max(u2, u3)), 0.0),
+                                             (double)(g.DNU - 1));
+                need = std::max(need, std::min((int)umax + 2, g.DNU - 1) - std::max((int)umin - 1, 0) + 1);
+            }
+        }
+    }
+    const size_t fixed = dyn_smem(0, vp, es2) + kStaticSmem;
+    const int cap = kSmemPerCta > fixed ? (int)((kSmemPerCta - fixed) / (4 * 2 * (size_t)vp)) : 0;
+    return std::max(2, std::min(need, cap));
+}
+
+cudaError_t launch_pv(const ProjSatArgs &a, float *out, int vp, cudaStream_t s)
+{
+    PrjIn in{a.prj, a.views, a.view_list, a.det, det_table_layout(a.DNU, a.DNV), a.DNU, a.DNV, a.dx};
+    const long long ncols = (long long)a.n * a.DNU;
+    const long long blocks = (ncols * 32 + 255) / 256;
+    if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    pv_kernel<<<(unsigned)blocks, 256, 0, s>>>(in, ncols, a.DNU, a.DNV, out, vp);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_back_t(const BackArgs &a, cudaStream_t s, int *launches)
+{
+    if (launches) ++*launches;
+    if (a.n <= 0) return cudaSuccess;
+    switch (vpt_of(a.DNV)) {
+    case 2: return launch_z<2>(a, s);
+    case 5: return launch_z<5>(a, s);
+    case 9: return launch_z<9>(a, s);
+    case 17: return launch_z<17>(a, s);
+    case 33: return launch_z<33>(a, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+} // namespace ctlab

@@ -133,6 +133,29 @@ cudaError_t launch_zt(const float *vol, const unsigned char *mask, int XN, int Y
 
 // Projection SAT: Q[p][u'][v'] of W = prj * L (L = slab path weight of the
 // view's driving axis) for n views of the list.
+// Projection rows weighted by the slab path length L of the view's driving
+// axis: W = prj * dx * |C - S| / |C_a - S_a| with C the cell centre.
+struct PrjIn {
+    const float *prj;
+    const DevView *views;
+    const int *list;
+    const double *det;
+    DetTable t;
+    int DNU, DNV;
+    double dx;
+    __device__ __forceinline__ float operator()(int plane, int u, int v) const
+    {
+        const DevView &V = views[list[plane]];
+        const double lx = det[t.off_ux + u], ly = det[t.off_uy + u];
+        const double cx = lx * V.c - ly * V.s, cy = lx * V.s + ly * V.c;
+        const float ex = (float)(cx - V.Sx), ey = (float)(cy - V.Sy);
+        const float ez = (float)(det[t.off_vz + v] + V.zP - V.Sz);
+        const float ea = V.xdrv ? ex : ey;
+        const float L = (float)dx * sqrtf(ex * ex + ey * ey + ez * ez) / fabsf(ea);
+        return __ldg(prj + ((long long)plane * DNU + u) * DNV + v) * L;
+    }
+};
+
 struct ProjSatArgs {
     const float *prj;     // [n][DNU][DNV]
     const DevView *views; // plan views
@@ -146,6 +169,9 @@ struct ProjSatArgs {
     int f32pair;
 };
 cudaError_t launch_proj_sat(const ProjSatArgs &a, ScanState st, int chunk, cudaStream_t s);
+// Projection v-prefixes (sat mode ZPREFIX): out[l][u][v'] = sum_{v<v'} W(l, u, v),
+// v' in [0, DNV] (entries up to the pitch vp repeat v' = DNV), FP64 sums in FP32.
+cudaError_t launch_pv(const ProjSatArgs &a, float *out, int vp, cudaStream_t s);
 // Diagnostics: a scan whose first chunk never publishes (see ctlab_debug_scan_stall).
 cudaError_t launch_scan_stall(const float *vol, int rows, int nk, void *out, ScanState st, int chunk,
                               unsigned spin_limit, cudaStream_t s);
@@ -234,8 +260,14 @@ struct BackArgs {
     float min_v, max_v;
     int rmax;             // staging-buffer SAT rows (back_staging_rows)
     int *err;             // device error word (bounded waits)
+    const float *pv;      // projection v-prefixes [n][DNU][vp] (sat mode ZPREFIX)
 };
 cudaError_t launch_back(const BackArgs &a, cudaStream_t s, int *launches);
+// Backprojector on projection v-prefixes (sat mode ZPREFIX).
+cudaError_t launch_back_t(const BackArgs &a, cudaStream_t s, int *launches);
+bool back_t_supported(int DNV);
+int back_t_pitch(int DNV);
+int back_t_staging_rows(const HostGeometry &g);
 bool back_supported(int DNV);
 int back_staging_rows(const HostGeometry &g, int vp);
 

@@ -22,6 +22,7 @@ struct LegacyCtx {
     std::mutex mu;
     ctlab_plan *plan = nullptr;
     unsigned long long key = 0;
+    int mode = -1;
     float *d_vol = nullptr;
     size_t vol_cap = 0;
     float *d_prj = nullptr;
@@ -87,21 +88,22 @@ int legacy_prepare(LegacyCtx &c, const ctlab_geometry &g, int gpunum)
         cudaError_t e = cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking);
         if (e != cudaSuccess) return cuda_status(e, "legacy stream");
     }
+    // SAT arithmetic of the cached plan: slice-major FP64-accumulated
+    // z-prefixes unless CTLAB_LEGACY_SAT selects 0 (2-D FP64 SAT) or 1
+    // (compensated FP32 pairs)
+    int mode = CTLAB_SAT_ZPREFIX;
+    if (const char *env = std::getenv("CTLAB_LEGACY_SAT")) {
+        const int m = std::atoi(env);
+        if (m == CTLAB_SAT_FP64 || m == CTLAB_SAT_F32PAIR || m == CTLAB_SAT_ZPREFIX) mode = m;
+    }
     const unsigned long long key = geometry_key(g);
-    if (!c.plan || c.key != key) {
+    if (!c.plan || c.key != key || c.mode != mode) {
         if (c.plan) ctlab_plan_destroy(c.plan);
         c.plan = nullptr;
-        // SAT arithmetic of the cached plan: slice-major FP64-accumulated
-        // z-prefixes unless CTLAB_LEGACY_SAT selects 0 (2-D FP64 SAT) or 1
-        // (compensated FP32 pairs)
-        int mode = CTLAB_SAT_ZPREFIX;
-        if (const char *env = std::getenv("CTLAB_LEGACY_SAT")) {
-            const int m = std::atoi(env);
-            if (m == CTLAB_SAT_FP64 || m == CTLAB_SAT_F32PAIR || m == CTLAB_SAT_ZPREFIX) mode = m;
-        }
         int rc = ctlab_plan_create(&g, gpunum, mode, &c.plan);
         if (rc != CTLAB_OK) return rc;
         c.key = key;
+        c.mode = mode;
     }
     const size_t nv = (size_t)g.XN * g.YN * g.ZN, np = (size_t)g.PN * g.DNU * g.DNV;
     int rc = grow(&c.d_vol, c.vol_cap, nv);

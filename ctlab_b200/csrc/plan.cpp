@@ -70,7 +70,7 @@ void plan_free(ctlab_plan *p)
 {
     if (!p) return;
     DeviceGuard g(p->device);
-    void *bufs[] = {p->d_views, p->d_det, p->d_all_views, p->d_list, p->d_sat_y, p->d_sat_x, p->d_zt_y, p->d_zt_x,
+    void *bufs[] = {p->d_views, p->d_det, p->d_all_views, p->d_list, p->d_sat_y, p->d_sat_x, p->d_zt_y, p->d_zt_x, p->d_pv,
                     p->d_q, p->d_ticket, p->d_flags, p->d_agg, p->d_pref, p->d_err,
                     p->d_groups_all, p->d_groups_scratch};
     for (void *b : bufs)
@@ -196,6 +196,12 @@ int plan_proj_sat(ctlab_plan *p, const int *d_list, int n, const float *d_prj, c
     a.out = p->d_q;
     a.vp = p->vp;
     a.f32pair = p->sat_mode == CTLAB_SAT_F32PAIR;
+    if (p->sat_mode == CTLAB_SAT_ZPREFIX) {
+        cudaError_t e = launch_pv(a, p->d_pv, p->vp, s);
+        if (e != cudaSuccess) return cuda_status(e, "projection v-prefixes");
+        ++p->last_launches;
+        return CTLAB_OK;
+    }
     ScanState st{p->d_ticket, p->d_flags, p->d_agg, p->d_pref, p->d_err};
     cudaError_t e = launch_proj_sat(a, st, kPrjChunk, s);
     if (e != cudaSuccess) return cuda_status(e, "projection SAT");
@@ -234,11 +240,13 @@ int plan_back_list(ctlab_plan *p, const int *d_list, int n, const unsigned char 
     a.max_v = max_v;
     a.rmax = p->back_rmax;
     a.err = p->d_err;
+    a.pv = p->d_pv;
     if (n == 0 && epilogue == BACK_PLAIN) {
         CTLAB_CUDA_TRY(cudaMemsetAsync(d_vol, 0, sizeof(float) * (size_t)g.XN * g.YN * g.ZN, s));
         return CTLAB_OK;
     }
-    cudaError_t e = launch_back(a, s, &p->last_launches);
+    cudaError_t e = p->sat_mode == CTLAB_SAT_ZPREFIX ? launch_back_t(a, s, &p->last_launches)
+                                                     : launch_back(a, s, &p->last_launches);
     if (e != cudaSuccess) return cuda_status(e, "DD3 backprojection kernel");
     return CTLAB_OK;
 }
@@ -315,7 +323,7 @@ int ctlab_plan_create(const ctlab_geometry *geom, int device, int sat_mode, ctla
     for (const auto &v : g.views) (v.xdrv ? p->need_x : p->need_y) = true;
     const bool zpre = sat_mode == CTLAB_SAT_ZPREFIX;
     p->zp = round_up(g.ZN + 1, 2);
-    p->vp = round_up(g.DNV + 1, 2);
+    p->vp = zpre ? back_t_pitch(g.DNV) : round_up(g.DNV + 1, 2);
     p->q_capacity = g.PN;
     if (zpre) {
         p->tst = proj_t_staging(g);
@@ -330,7 +338,7 @@ int ctlab_plan_create(const ctlab_geometry *geom, int device, int sat_mode, ctla
         p->proj_cmax = st.cmax;
         p->proj_nbuf = st.nbuf;
     }
-    if (g.flat_uniform) p->back_rmax = back_staging_rows(g, p->vp);
+    if (g.flat_uniform) p->back_rmax = zpre ? back_t_staging_rows(g) : back_staging_rows(g, p->vp);
 
     long long &bytes = p->bytes;
     cudaError_t e = cudaSuccess;
@@ -350,7 +358,9 @@ int ctlab_plan_create(const ctlab_geometry *geom, int device, int sat_mode, ctla
         if (p->need_y) chk(dmalloc((char **)&p->d_sat_y, esz * (size_t)g.YN * (g.XN + 1) * p->zp, bytes));
         if (p->need_x) chk(dmalloc((char **)&p->d_sat_x, esz * (size_t)g.XN * (g.YN + 1) * p->zp, bytes));
     }
-    if (back_supported(g.DNV) && g.flat_uniform)
+    if (zpre && back_t_supported(g.DNV) && g.flat_uniform)
+        chk(dmalloc(&p->d_pv, (size_t)g.PN * g.DNU * p->vp, bytes));
+    else if (!zpre && back_supported(g.DNV) && g.flat_uniform)
         chk(dmalloc((char **)&p->d_q, esz * (size_t)g.PN * (g.DNU + 1) * p->vp, bytes));
     else
         p->q_capacity = 0;
@@ -363,7 +373,7 @@ int ctlab_plan_create(const ctlab_geometry *geom, int device, int sat_mode, ctla
     };
     if (p->need_y && !zpre) need(g.YN, g.XN, g.ZN, kVolChunk);
     if (p->need_x && !zpre) need(g.XN, g.YN, g.ZN, kVolChunk);
-    if (p->q_capacity) need(g.PN, g.DNU, g.DNV, kPrjChunk);
+    if (p->q_capacity && !zpre) need(g.PN, g.DNU, g.DNV, kPrjChunk);
     chk(dmalloc(&p->d_ticket, 1, bytes));
     chk(dmalloc(&p->d_flags, tiles, bytes));
     chk(dmalloc(&p->d_agg, state, bytes));

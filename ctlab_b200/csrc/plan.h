@@ -23,6 +23,7 @@ struct ctlab_plan {
     ctlab::ProjTStaging tst;                    // z-prefix projector staging
     int zp = 0;                 // z stride of the volume SATs
     void *d_q = nullptr; // projection SATs [q_capacity][DNU+1][vp]
+    float *d_pv = nullptr; // projection v-prefixes [q_capacity][DNU][vp] (sat mode ZPREFIX)
     int vp = 0;
     int q_capacity = 0;
     int proj_cmax = 2;  // projector staging columns

@@ -123,28 +123,6 @@ struct VolInX { // SAT_x: plane = x slice i, s = y index, k = z
     }
 };
 
-// Projection rows weighted by the slab path length L of the view's driving
-// axis: W = prj * dx * |C - S| / |C_a - S_a| with C the cell centre.
-struct PrjIn {
-    const float *prj;
-    const DevView *views;
-    const int *list;
-    const double *det;
-    DetTable t;
-    int DNU, DNV;
-    double dx;
-    __device__ __forceinline__ float operator()(int plane, int u, int v) const
-    {
-        const DevView &V = views[list[plane]];
-        const double lx = det[t.off_ux + u], ly = det[t.off_uy + u];
-        const double cx = lx * V.c - ly * V.s, cy = lx * V.s + ly * V.c;
-        const float ex = (float)(cx - V.Sx), ey = (float)(cy - V.Sy);
-        const float ez = (float)(det[t.off_vz + v] + V.zP - V.Sz);
-        const float ea = V.xdrv ? ex : ey;
-        const float L = (float)dx * sqrtf(ex * ex + ey * ey + ez * ez) / fabsf(ea);
-        return __ldg(prj + ((long long)plane * DNU + u) * DNV + v) * L;
-    }
-};
 
 template <class In, class T, int KPT>
 __global__ void __launch_bounds__(kThreads)

@@ -92,7 +92,7 @@ class Plan:
     """Device-resident plan (``ctlab_plan``): geometry tables and SAT
     workspaces on one GPU; calls are ordered on the given CUDA stream."""
 
-    def __init__(self, g: DD3Geometry, device: int = 0, sat_mode: int = _lib.CTLAB_SAT_FP64):
+    def __init__(self, g: DD3Geometry, device: int = 0, sat_mode: int = _lib.CTLAB_SAT_ZPREFIX):
         self.lib = load()
         self.g = g
         self.device = device

@@ -225,8 +225,12 @@ def test_gpu_phantom_matches_oracle_phantom(torch_cuda):
     assert bad.mean() < 1e-4  # float vs double inside-tests on the surfaces only
 
 
-def test_legacy_host_entry_points_equal_plan_path(torch_cuda):
+@pytest.mark.parametrize("sat_mode", [cb.CTLAB_SAT_ZPREFIX, cb.CTLAB_SAT_FP64])
+def test_legacy_host_entry_points_equal_plan_path(torch_cuda, sat_mode, monkeypatch):
+    """DD3Proj_gpu / DD3Back_gpu (host pointers) equal the device plan path bit for
+    bit; CTLAB_LEGACY_SAT selects the legacy calls' SAT arithmetic."""
     torch = torch_cuda
+    monkeypatch.setenv("CTLAB_LEGACY_SAT", str(sat_mode))
     g = make_case("odd_offsets")
     vol = phantom(g)
     mask = (np.random.default_rng(4).random(g.XN * g.YN) > 0.3).astype(np.uint8)
@@ -234,7 +238,7 @@ def test_legacy_host_entry_points_equal_plan_path(torch_cuda):
     cb.DD3Proj_gpu(**g.args(), hvol=vol, hprj=hp, mask=mask, gpunum=0, prjMode=0)
     hb = np.zeros(g.vol_shape, np.float32)
     cb.DD3Back_gpu(**g.args(), hvol=hb, hprj=hp, mask=mask, gpunum=0, squared=1, prjMode=0)
-    with cb.Plan(g) as plan:
+    with cb.Plan(g, sat_mode=sat_mode) as plan:
         out = torch.zeros(g.prj_shape, dtype=torch.float32, device="cuda")
         plan.proj(dev(torch, vol), out, mask=dev(torch, mask))
         vb = torch.zeros(g.vol_shape, dtype=torch.float32, device="cuda")

@@ -34,7 +34,7 @@ def test_noalloc_volume_sat_matches_plan_path_on_two_calls(torch_cuda):
     vol = torch.from_numpy(rng.random(g.vol_shape).astype(np.float32)).cuda()
     mask = torch.from_numpy((rng.random(g.XN * g.YN) > 0.2).astype(np.uint8)).cuda()
     stream = torch.cuda.current_stream().cuda_stream
-    with cb.Plan(g) as plan:
+    with cb.Plan(g, sat_mode=cb.CTLAB_SAT_FP64) as plan:  # the 2-D FP64 SAT the entry point also builds
         plan.volume_sat(vol, mask)
         refs = {}
         for o in (0, 1):
