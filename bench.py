@@ -275,7 +275,11 @@ def run_ours(args):
     t_proj, t_back = float(np.mean(proj_k)), float(np.mean(back_k))
     peak, peak_kind = peaks()
     alg = 8.0 * vv + 4.0 * g.PN * g.DNU * g.DNV  # bytes per launch (proj or back)
-    dom = ("dd3_proj_zp_kernel" if args.sat == "zprefix" else "dd3_proj_kernel") if t_proj >= t_back else "dd3_back_kernel"
+    zp = args.sat == "zprefix"
+    if t_proj >= t_back:
+        dom = "dd3_proj_t_kernel" if zp else "dd3_proj_kernel"
+    else:
+        dom = "dd3_back_t_kernel" if zp else "dd3_back_kernel"
     t_dom = max(t_proj, t_back)
     achieved = alg / (t_dom * 1e-3) / 1e9
     traffic = None
