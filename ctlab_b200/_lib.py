@@ -24,6 +24,7 @@ CTLAB_ERR_INTERNAL = 6
 CTLAB_SAT_FP64 = 0
 CTLAB_SAT_F32PAIR = 1
 CTLAB_SAT_ZPREFIX = 2
+CTLAB_CG_FR, CTLAB_CG_PRP, CTLAB_CG_CW, CTLAB_CG_DI, CTLAB_CG_DY = range(5)
 
 _ERR_NAMES = {
     CTLAB_ERR_INVALID_ARG: "invalid argument",
@@ -89,6 +90,7 @@ _SIGNATURES = {
                                 C.c_float, C.c_float, _fp, _vp]),
     "ctlab_fista_tv": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_float, C.c_float, C.c_float,
                                  C.c_float, _fp, _vp]),
+    "ctlab_cg": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int, _fp, _vp]),
     "ctlab_tv_gradient": (C.c_int, [_vp, _vp, C.c_int, C.c_int, C.c_int, C.c_float, _vp]),
     "ctlab_fista_step": (C.c_int, [_vp, _vp, C.c_float, C.c_float, C.c_longlong, C.c_float,
                                    C.c_float, _vp]),

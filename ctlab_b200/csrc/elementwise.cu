@@ -124,6 +124,28 @@ __global__ void resid2_kernel(const float *meas, const float *est, long long n, 
     }
 }
 
+// acc += sum a*b in FP64 (block partial sums, one atomic per block)
+__global__ void dot_kernel(const float *a, const float *b, long long n, double *acc)
+{
+    double t = 0.0;
+    GRID_STRIDE(i, n) { t += (double)a[i] * (double)b[i]; }
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    __shared__ double sw[kT / 32];
+    if ((threadIdx.x & 31) == 0) sw[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tt = 0;
+        for (int w = 0; w < kT / 32; ++w) tt += sw[w];
+        atomicAdd(acc, tt);
+    }
+}
+
+// y = alpha * x + beta * y
+__global__ void axpby_kernel(float *y, float alpha, const float *x, float beta, long long n)
+{
+    GRID_STRIDE(i, n) { y[i] = fmaf(alpha, x[i], beta * y[i]); }
+}
+
 // Smoothed isotropic TV gradient, forward differences, replicated borders;
 // the 3-D GradientOfTV_GPU of src/differentialFuncs.hpp:491-501.  One
 // thread per voxel, z fastest (coalesced); neighbours come from L1/L2.
@@ -252,6 +274,16 @@ cudaError_t launch_gather_views(const float *src, const int *list, int nv, long 
 cudaError_t launch_resid2(const float *meas, const float *est, long long n, double *acc, cudaStream_t s)
 {
     resid2_kernel<<<grid_for(n), kT, 0, s>>>(meas, est, n, acc);
+    return cudaGetLastError();
+}
+cudaError_t launch_dot(const float *a, const float *b, long long n, double *acc, cudaStream_t s)
+{
+    dot_kernel<<<grid_for(n), kT, 0, s>>>(a, b, n, acc);
+    return cudaGetLastError();
+}
+cudaError_t launch_axpby(float *y, float alpha, const float *x, float beta, long long n, cudaStream_t s)
+{
+    axpby_kernel<<<grid_for(n), kT, 0, s>>>(y, alpha, x, beta, n);
     return cudaGetLastError();
 }
 cudaError_t launch_phantom(float *vol, int XN, int YN, int ZN, float dx, float dz, float cx, float cy, float cz,

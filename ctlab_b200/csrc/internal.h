@@ -292,6 +292,10 @@ cudaError_t launch_gather_views(const float *src, const int *list, int n, long l
 // sum of squares of (a - b) and of a (double accumulators)
 cudaError_t launch_resid2(const float *meas, const float *est, long long n, double *acc, cudaStream_t s);
 
+// acc += sum a*b (FP64); y = alpha x + beta y
+cudaError_t launch_dot(const float *a, const float *b, long long n, double *acc, cudaStream_t s);
+cudaError_t launch_axpby(float *y, float alpha, const float *x, float beta, long long n, cudaStream_t s);
+
 cudaError_t launch_phantom(float *vol, int XN, int YN, int ZN, float dx, float dz, float cx, float cy,
                            float cz, const float *ell_dev, int n_ell, int clamp_nonneg, cudaStream_t s);
 

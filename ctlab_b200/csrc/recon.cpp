@@ -7,6 +7,8 @@
 // fused into its epilogue.
 #include <cmath>
 #include <cstring>
+#include <initializer_list>
+#include <utility>
 #include <vector>
 
 #include "plan.h"
@@ -232,6 +234,115 @@ int ctlab_fista_tv(ctlab_plan *plan, float *d_x, const float *d_meas, const unsi
         }
     }
     CTLAB_CUDA_TRY(cudaMemcpyAsync(d_x, xp, sizeof(float) * nv, cudaMemcpyDeviceToDevice, s));
+    rc = plan_check_device_error(plan, s);
+    return rc == CTLAB_OK ? ok() : rc;
+}
+
+int ctlab_cg(ctlab_plan *plan, float *d_x, const float *d_meas, const unsigned char *d_mask, int iter_num, int method,
+             float *h_resid, void *stream)
+{
+    if (!plan || !d_x || !d_meas) return set_status(CTLAB_ERR_INVALID_ARG, "null plan, image or projection");
+    if (iter_num < 0) return set_status(CTLAB_ERR_INVALID_ARG, "iter_num must be >= 0");
+    if (method < CTLAB_CG_FR || method > CTLAB_CG_DY) return set_status(CTLAB_ERR_INVALID_ARG, "unknown CG beta method");
+    const HostGeometry &g = plan->g;
+    if (!g.flat_uniform || plan->q_capacity == 0)
+        return set_status(CTLAB_ERR_UNSUPPORTED, "CG needs a flat detector with uniform u and v pitch");
+    std::lock_guard<std::mutex> lk(plan->mu);
+    DeviceGuard dg(plan->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    plan->last_launches = 0;
+    const long long nd = (long long)g.DNU * g.DNV * g.PN;
+    const long long nv = (long long)g.XN * g.YN * g.ZN;
+    const int *all = plan->d_all_views;
+
+    DevBuf d_r, d_q, d_g, d_gn, d_d, d_acc;
+    int rc = alloc(d_r, sizeof(float) * nd);
+    if (rc == CTLAB_OK) rc = alloc(d_q, sizeof(float) * nd);
+    if (rc == CTLAB_OK) rc = alloc(d_g, sizeof(float) * nv);
+    if (rc == CTLAB_OK) rc = alloc(d_gn, sizeof(float) * nv);
+    if (rc == CTLAB_OK) rc = alloc(d_d, sizeof(float) * nv);
+    if (rc == CTLAB_OK) rc = alloc(d_acc, sizeof(double) * 4);
+    if (rc != CTLAB_OK) return rc;
+    float *r = d_r.as<float>(), *q = d_q.as<float>(), *gk = d_g.as<float>(), *gn = d_gn.as<float>(),
+          *dk = d_d.as<float>();
+    double *acc = d_acc.as<double>();
+
+    // A v (masked volume) and A^T p (masked), over all views
+    auto proj = [&](const float *vol, float *out) {
+        int e = plan_volume_sat(plan, vol, d_mask, s);
+        if (e == CTLAB_OK)
+            e = plan_proj_list(plan, all, g.PN, plan_all_groups(plan), out, s, PROJ_PLAIN, nullptr, nullptr, nullptr);
+        return e;
+    };
+    auto back = [&](const float *prj, float *out) {
+        int e = plan_proj_sat(plan, all, g.PN, prj, s);
+        if (e == CTLAB_OK) e = plan_back_list(plan, all, g.PN, d_mask, out, s, BACK_PLAIN, nullptr, 1.f, 0, 0.f, 0.f);
+        return e;
+    };
+    // FP64 dot products of up to 4 (a, b, n) terms, read back
+    struct Dot {
+        const float *a, *b;
+        long long n;
+    };
+    auto dots = [&](std::initializer_list<Dot> terms, double *out) {
+        CTLAB_CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(double) * 4, s));
+        int k = 0;
+        for (const Dot &t : terms) CTLAB_CUDA_TRY(launch_dot(t.a, t.b, t.n, acc + k++, s));
+        CTLAB_CUDA_TRY(cudaMemcpyAsync(out, acc, sizeof(double) * k, cudaMemcpyDeviceToHost, s));
+        CTLAB_CUDA_TRY(cudaStreamSynchronize(s));
+        return (int)CTLAB_OK;
+    };
+
+    double bb = 0.0;
+    rc = dots({{d_meas, d_meas, nd}}, &bb);
+    // r = A x - b, g = A^T r, d = -g
+    if (rc == CTLAB_OK) rc = proj(d_x, r);
+    if (rc == CTLAB_OK) rc = launch_axpby(r, -1.f, d_meas, 1.f, nd, s) == cudaSuccess ? CTLAB_OK : CTLAB_ERR_CUDA;
+    if (rc == CTLAB_OK) rc = back(r, gk);
+    if (rc == CTLAB_OK) rc = launch_axpby(dk, -1.f, gk, 0.f, nv, s) == cudaSuccess ? CTLAB_OK : CTLAB_ERR_CUDA;
+    double gg = 0.0;
+    if (rc == CTLAB_OK) rc = dots({{gk, gk, nv}}, &gg);
+    if (rc != CTLAB_OK) return rc;
+    for (int it = 0; it < iter_num; ++it) {
+        // exact line search along d for 1/2 ||A x - b||^2
+        rc = proj(dk, q);
+        double h[4];
+        if (rc == CTLAB_OK) rc = dots({{q, q, nd}, {gk, dk, nv}}, h);
+        if (rc != CTLAB_OK) return rc;
+        const double qq = h[0], gd = h[1];
+        if (!(qq > 0.0) || !(gg > 0.0)) {
+            for (int k = it; k < iter_num && h_resid; ++k) h_resid[k] = k > 0 ? h_resid[k - 1] : 0.f;
+            break;
+        }
+        const float alpha = (float)(-gd / qq);
+        CTLAB_CUDA_TRY(launch_axpby(d_x, alpha, dk, 1.f, nv, s));
+        CTLAB_CUDA_TRY(launch_axpby(r, alpha, q, 1.f, nd, s));
+        rc = back(r, gn);
+        double gng = 0.0, gng_old = 0.0, dgn = 0.0, rr = 0.0;
+        if (rc == CTLAB_OK) rc = dots({{gn, gn, nv}, {gn, gk, nv}, {dk, gn, nv}, {r, r, nd}}, h);
+        if (rc != CTLAB_OK) return rc;
+        rr = h[3];
+        gng = h[0];
+        gng_old = h[1];
+        dgn = h[2];
+        // beta of the chosen update (Fletcher-Reeves, Polak-Ribiere-Polyak,
+        // Crowder-Wolfe / Hestenes-Stiefel, Dixon, Dai-Yuan)
+        const double y_d = dgn - gd; // d^T (g_new - g)
+        double beta = 0.0;
+        switch (method) {
+        case CTLAB_CG_FR: beta = gng / gg; break;
+        case CTLAB_CG_PRP: beta = (gng - gng_old) / gg; break;
+        case CTLAB_CG_CW: beta = y_d != 0.0 ? (gng - gng_old) / y_d : 0.0; break;
+        case CTLAB_CG_DI: beta = gd != 0.0 ? -gng / gd : 0.0; break;
+        case CTLAB_CG_DY: beta = y_d != 0.0 ? gng / y_d : 0.0; break;
+        }
+        if (!std::isfinite(beta)) beta = 0.0;
+        CTLAB_CUDA_TRY(launch_axpby(dk, -1.f, gn, (float)beta, nv, s));
+        std::swap(gk, gn);
+        gg = gng;
+        plan->last_launches += 4;
+        if (h_resid) h_resid[it] = (float)(bb > 0 ? std::sqrt(rr / bb) : 0.0);
+    }
     rc = plan_check_device_error(plan, s);
     return rc == CTLAB_OK ? ok() : rc;
 }

@@ -189,6 +189,13 @@ class Plan:
             None if res is None else res.ctypes.data_as(_fp), self._stream(stream)))
         return None if res is None else res[:iter_num]
 
+    def cg(self, x, meas, mask=None, iter_num: int = 10, method: int = 0, residuals: bool = False, stream=None):
+        """Conjugate gradient for min ||A x - b||^2 (ctlab_cg); method is a CTLAB_CG_* beta rule."""
+        res = np.zeros(max(iter_num, 1), np.float32) if residuals else None
+        check(self.lib.ctlab_cg(self.handle, self._p(x), self._p(meas), self._p(mask), iter_num, method,
+                                None if res is None else res.ctypes.data_as(_fp), self._stream(stream)))
+        return None if res is None else res[:iter_num]
+
     def fista_tv(self, x, meas, mask=None, iter_num: int = 50, tv_lambda: float = 1e-4, tv_eps: float = 1e-8,
                  min_v: float = -2000.0, max_v: float = 6000.0, residuals: bool = False, stream=None):
         res = np.zeros(max(iter_num, 1), np.float32) if residuals else None

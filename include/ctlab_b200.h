@@ -207,6 +207,22 @@ int ctlab_fista_tv(ctlab_plan *plan, float *d_x, const float *d_meas,
                    const unsigned char *d_mask, int iter_num, float tv_lambda, float tv_eps,
                    float min_v, float max_v, float *h_resid, void *stream);
 
+/* Nonlinear conjugate gradient for min 1/2 ||A x - b||^2 over the masked
+ * volume, all views, exact line search along each direction; the beta
+ * update is CTLAB_CG_FR (Fletcher-Reeves), _PRP (Polak-Ribiere-Polyak), _CW
+ * (Crowder-Wolfe, the Hestenes-Stiefel form), _DI (Dixon) or _DY
+ * (Dai-Yuan), the members of CGMethod, src/DD3_GPU_recon.h:14-19.  d_x holds
+ * the initial image and receives the result; h_resid (may be NULL) receives
+ * ||A x_k - b|| / ||b|| after each iteration.  Replaces the GPU body of CG,
+ * src/DD3_GPU_recon.h:98-103. */
+#define CTLAB_CG_FR 0
+#define CTLAB_CG_PRP 1
+#define CTLAB_CG_CW 2
+#define CTLAB_CG_DI 3
+#define CTLAB_CG_DY 4
+int ctlab_cg(ctlab_plan *plan, float *d_x, const float *d_meas, const unsigned char *d_mask, int iter_num,
+             int method, float *h_resid, void *stream);
+
 /* Smoothed isotropic TV gradient of d_f into d_g (both (Z,X,Y)).  The 3-D
  * form of GradientOfTV_GPU, src/differentialFuncs.hpp:491-501. */
 int ctlab_tv_gradient(const float *d_f, float *d_g, int XN, int YN, int ZN, float eps,

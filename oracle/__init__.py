@@ -176,6 +176,41 @@ def fista_tv(g, x0, prj, mask=None, iter_num=3, tv_lambda=1e-4, tv_eps=1e-8, min
     return x
 
 
+def cg(g, x0, prj, mask=None, iter_num=3, method=0):
+    """Nonlinear conjugate gradient for 1/2 ||A x - b||^2 with an exact line
+    search along each direction (FP64 vectors; A, A^T = dd3_proj, dd3_back).
+    method: 0 Fletcher-Reeves, 1 Polak-Ribiere-Polyak, 2 Crowder-Wolfe
+    (Hestenes-Stiefel), 3 Dixon, 4 Dai-Yuan -- the beta rules named by
+    CGMethod, src/DD3_GPU_recon.h:14-19, as published in the nonlinear CG
+    literature.  Returns the image and ||A x_k - b|| / ||b|| per iteration."""
+    A = lambda v: dd3_proj(g, v, mask).astype(np.float64)
+    At = lambda r: dd3_back(g, r, mask).astype(np.float64)
+    x = np.asarray(x0, np.float64).copy()
+    b = np.asarray(prj, np.float64)
+    r = A(x) - b
+    gk = At(r)
+    d = -gk
+    gg = float(np.vdot(gk, gk))
+    res = []
+    for _ in range(iter_num):
+        q = A(d)
+        qq, gd = float(np.vdot(q, q)), float(np.vdot(gk, d))
+        if qq <= 0 or gg <= 0:
+            break
+        alpha = -gd / qq
+        x += alpha * d
+        r += alpha * q
+        gn = At(r)
+        gng, gng_old, dgn = float(np.vdot(gn, gn)), float(np.vdot(gn, gk)), float(np.vdot(d, gn))
+        yd = dgn - gd
+        beta = [gng / gg, (gng - gng_old) / gg, (gng - gng_old) / yd if yd else 0.0,
+                -gng / gd if gd else 0.0, gng / yd if yd else 0.0][method]
+        d = -gn + beta * d
+        gk, gg = gn, gng
+        res.append(float(np.linalg.norm(r) / np.linalg.norm(b)))
+    return x.astype(np.float32), np.array(res)
+
+
 def set_threads(n: int) -> None:
     load().orc_set_num_threads(n)
 
