@@ -206,6 +206,7 @@ struct ProjArgs {
     int t_cb, t_kb, t_kr;     // stage: [t_kr][t_cb] floats, TMA boxes of t_kb rows
     int t_nstage, t_rb, t_ep, t_gtab; // stages, consumer warps per view, z-boundary pitch, table views
     int t_zs;                         // detector rows split over t_zs CTAs
+    int t_nr;                         // detector rows per consumer warp (t_nr * t_rb rows per CTA)
 };
 
 // Views of one launch grouped by driving axis and angle, G per CTA.
@@ -232,7 +233,9 @@ struct ProjTStaging {
     size_t smem = 0;
     bool ok = false;
 };
-ProjTStaging proj_t_staging(const HostGeometry &g);
+// gcap limits the views per CTA (launches whose views group one by one use
+// a staging planned with gcap = 1).
+ProjTStaging proj_t_staging(const HostGeometry &g, int gcap = 16);
 ProjGroups proj_t_make_groups(const HostGeometry &g, const std::vector<int> &list, const ProjTStaging &st);
 cudaError_t launch_proj_t(const ProjArgs &a, const ProjTStaging &st, const CUtensorMap &tmy, const CUtensorMap &tmx,
                           cudaStream_t s, int *launches);

@@ -159,7 +159,10 @@ int plan_proj_list(ctlab_plan *p, const int *d_list, int n, const GroupTab &gt, 
     a.ngroups = gt.ngroups;
     a.G = gt.G;
     if (p->sat_mode == CTLAB_SAT_ZPREFIX) {
-        const ProjTStaging &st = p->tst;
+        // view lists that group one view per CTA (ordered subsets of spread
+        // views) run with the staging planned for single views
+        const bool single = gt.G == 1 && p->tst1.ok && p->tst.G > 1;
+        const ProjTStaging &st = single ? p->tst1 : p->tst;
         a.zt_y = p->d_zt_y;
         a.zt_x = p->d_zt_x;
         a.zt_rs_y = p->zt_rs_y;
@@ -168,11 +171,20 @@ int plan_proj_list(ctlab_plan *p, const int *d_list, int n, const GroupTab &gt, 
         a.t_kb = st.KB;
         a.t_kr = st.KR;
         a.t_nstage = st.nstage;
-        a.t_rb = st.RB;
+        // launches whose groups hold fewer views than planned keep the rows
+        // per CTA and split them over more warps (rows per warp >= 8)
+        int nr = st.NR, rb = st.RB;
+        while (gt.G * rb * 2 <= 16 && nr >= 16) {
+            nr /= 2;
+            rb *= 2;
+        }
+        a.t_rb = rb;
+        a.t_nr = nr;
         a.t_zs = st.ZS;
         a.t_ep = st.EP;
         a.t_gtab = st.G;
-        cudaError_t e = launch_proj_t(a, st, p->tm_y, p->tm_x, s, &p->last_launches);
+        cudaError_t e = single ? launch_proj_t(a, st, p->tm1_y, p->tm1_x, s, &p->last_launches)
+                               : launch_proj_t(a, st, p->tm_y, p->tm_x, s, &p->last_launches);
         if (e != cudaSuccess) return cuda_status(e, "DD3 projection kernel (z-prefix)");
         return CTLAB_OK;
     }
@@ -327,6 +339,7 @@ int ctlab_plan_create(const ctlab_geometry *geom, int device, int sat_mode, ctla
     p->q_capacity = g.PN;
     if (zpre) {
         p->tst = proj_t_staging(g);
+        p->tst1 = proj_t_staging(g, 1);
         if (!p->tst.ok) {
             delete p;
             return set_status(CTLAB_ERR_UNSUPPORTED, "DNV beyond the z-prefix projector's tiles");
@@ -391,6 +404,13 @@ int ctlab_plan_create(const ctlab_geometry *geom, int device, int sat_mode, ctla
         if (p->need_y) rc2 = encode_zt_map(&p->tm_y, p->d_zt_y, g.XN, g.ZN, g.YN, p->zt_rs_y, p->tst.CB, p->tst.KB);
         if (rc2 == CTLAB_OK && p->need_x)
             rc2 = encode_zt_map(&p->tm_x, p->d_zt_x, g.YN, g.ZN, g.XN, p->zt_rs_x, p->tst.CB, p->tst.KB);
+        if (rc2 == CTLAB_OK && p->tst1.ok && p->tst1.CB > 0) {
+            if (p->need_y) rc2 = encode_zt_map(&p->tm1_y, p->d_zt_y, g.XN, g.ZN, g.YN, p->zt_rs_y, p->tst1.CB, p->tst1.KB);
+            if (rc2 == CTLAB_OK && p->need_x)
+                rc2 = encode_zt_map(&p->tm1_x, p->d_zt_x, g.YN, g.ZN, g.XN, p->zt_rs_x, p->tst1.CB, p->tst1.KB);
+        } else {
+            p->tst1.ok = false;
+        }
         if (rc2 != CTLAB_OK) {
             plan_free(p);
             return rc2;

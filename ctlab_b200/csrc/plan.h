@@ -21,6 +21,8 @@ struct ctlab_plan {
     int zt_rs_y = 0, zt_rs_x = 0;               // their row strides (floats)
     CUtensorMap tm_y, tm_x;                     // TMA maps of the z-prefix arrays
     ctlab::ProjTStaging tst;                    // z-prefix projector staging
+    CUtensorMap tm1_y, tm1_x;                   // the same for launches of single-view groups
+    ctlab::ProjTStaging tst1;
     int zp = 0;                 // z stride of the volume SATs
     void *d_q = nullptr; // projection SATs [q_capacity][DNU+1][vp]
     float *d_pv = nullptr; // projection v-prefixes [q_capacity][DNU][vp] (sat mode ZPREFIX)

@@ -581,14 +581,14 @@ int env_int(const char *name, int dflt)
 
 } // namespace
 
-ProjTStaging proj_t_staging(const HostGeometry &g)
+ProjTStaging proj_t_staging(const HostGeometry &g, int gcap)
 {
     ProjTStaging st;
     st.ok = false;
     // CTLAB_PROJT_GMAX caps the views per CTA (1..16), CTLAB_PROJT_ZS fixes
     // the row split (1, 2, 4), CTLAB_PROJT_NSTAGE the stage depth (2..4),
     // CTLAB_PROJT_CBMAX caps the staged columns
-    const int gmax = std::max(1, std::min(env_int("CTLAB_PROJT_GMAX", 8), kTMaxG));
+    const int gmax = std::max(1, std::min(std::min(env_int("CTLAB_PROJT_GMAX", 8), kTMaxG), gcap));
     const int want_zs = env_int("CTLAB_PROJT_ZS", 0);
     const int want_stage = env_int("CTLAB_PROJT_NSTAGE", 0);
     const int cbmax = std::min(env_int("CTLAB_PROJT_CBMAX", 256), 256);
@@ -609,9 +609,9 @@ ProjTStaging proj_t_staging(const HostGeometry &g)
             if (want_zs && ZS != want_zs) continue;
             if (!want_zs && ZS > 1 && g.DNV < 16 * ZS) continue;
             const int rows = (g.DNV + ZS - 1) / ZS; // detector rows per CTA
-            // rows per consumer warp: 4..32, the row blocks of G views filling
-            // at most 16 warps
-            int NR = 4;
+            // rows per consumer warp: 8..32 (4 for tiny detectors), the row
+            // blocks of G views filling at most 16 warps
+            int NR = rows >= 64 ? 8 : 4;
             while ((rows + NR - 1) / NR * G > kTMaxCWarps && NR < 32) NR *= 2;
             const int RB = (rows + NR - 1) / NR;
             if (RB * G > kTMaxCWarps) continue;
@@ -682,7 +682,8 @@ cudaError_t launch_proj_t(const ProjArgs &a, const ProjTStaging &st, const CUten
     if (a.ngroups > 65535 || a.G > st.G || a.G * a.t_rb > kTMaxCWarps) return cudaErrorInvalidConfiguration;
     if (launches) ++*launches;
     const size_t sm = smem_bytes(st);
-    switch (st.NR) {
+    if (a.t_nr * a.t_rb != st.NR * st.RB) return cudaErrorInvalidConfiguration;
+    switch (a.t_nr) {
     case 4: return launch_t_nr<4>(a, tmy, tmx, sm, s);
     case 8: return launch_t_nr<8>(a, tmy, tmx, sm, s);
     case 16: return launch_t_nr<16>(a, tmy, tmx, sm, s);
