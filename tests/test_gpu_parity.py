@@ -80,7 +80,7 @@ def test_projection_matches_oracle(torch_cuda, name, sat_mode):
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
-@pytest.mark.parametrize("sat_mode", [cb.CTLAB_SAT_FP64, cb.CTLAB_SAT_F32PAIR])
+@pytest.mark.parametrize("sat_mode", [cb.CTLAB_SAT_FP64, cb.CTLAB_SAT_F32PAIR, cb.CTLAB_SAT_ZPREFIX])
 def test_backprojection_matches_oracle(torch_cuda, name, sat_mode):
     torch = torch_cuda
     g = make_case(name)
