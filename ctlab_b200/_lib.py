@@ -91,6 +91,15 @@ _SIGNATURES = {
     "ctlab_fista_tv": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_float, C.c_float, C.c_float,
                                  C.c_float, _fp, _vp]),
     "ctlab_cg": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int, _fp, _vp]),
+    "ctlab_cnn_conv": (C.c_int, [_vp, C.c_int, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp,
+                                 _vp, _vp, _vp]),
+    "ctlab_cnn_wgrad": (C.c_int, [_vp, C.c_int, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp]),
+    "ctlab_cnn_pack": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _vp, C.c_int, C.c_float, _vp, _vp, _vp, _vp,
+                                 _vp]),
+    "ctlab_cnn_unpack": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _vp, C.c_int, C.c_float, _vp, _vp]),
+    "ctlab_cnn_loss_grad": (C.c_int, [_vp, _vp, C.c_longlong, _vp, _vp, _vp]),
+    "ctlab_cnn_adam": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float,
+                                 C.c_int, _vp, _vp, _vp]),
     "ctlab_tv_gradient": (C.c_int, [_vp, _vp, C.c_int, C.c_int, C.c_int, C.c_float, _vp]),
     "ctlab_fista_step": (C.c_int, [_vp, _vp, C.c_float, C.c_float, C.c_longlong, C.c_float,
                                    C.c_float, _vp]),

@@ -243,6 +243,55 @@ int ctlab_sart_back_weight(float *d_vol, float *d_recon, const float *d_col_sum,
                            void *stream);
 
 /* ---------------------------------------------------------------------- */
+/* Learned warm start: 2.5D residual CNN kernels (no counterpart in the   */
+/* reference; the network that warm-starts OS-SART)                       */
+/* ---------------------------------------------------------------------- */
+
+/* Convolution epilogues. */
+#define CTLAB_CNN_EPI_RELU 0     /* out = bf16(relu(conv + bias)) */
+#define CTLAB_CNN_EPI_MASK 1     /* out = bf16(conv) where mask > 0, else 0 (backward through ReLU) */
+#define CTLAB_CNN_EPI_RESIDUAL 2 /* out_f32 = conv[channel 0] + bias[0] + center (output layer) */
+
+/* 3x3 convolution, stride 1, zero padding, on NHWC BF16 tensors
+ * d_in [B][H][W][ci] with weights d_w [co][9][ci] (tap = 3*dy + dx), FP32
+ * accumulation on the tensor cores.  (ci, co) is (16, 64), (64, 64) or
+ * (64, 16).  The data gradient of a layer is this convolution with the
+ * flipped, channel-transposed weights (ctlab_cnn_adam writes them) and the
+ * MASK epilogue. */
+int ctlab_cnn_conv(const void *d_in, int ci, const void *d_w, const float *d_bias, int co, int B, int H, int W,
+                   int epi, void *d_out, const void *d_mask, float *d_out_f32, const float *d_center,
+                   void *stream);
+
+/* Weight (and, with d_db, bias) gradients of a convolution, accumulated:
+ * d_dw [co][9][ci] += sum_p dpre[p][co] * act[p + tap][ci]. */
+int ctlab_cnn_wgrad(const void *d_dpre, int co, const void *d_act, int ci, int B, int H, int W, float *d_dw,
+                    float *d_db, void *stream);
+
+/* Network inputs for the z slices d_z[nb] of a (Z,X,Y) volume: NHWC BF16
+ * [nb][YN][XN][16] holding slices z-2..z+2 (clamped) times scale, the FP32
+ * centre slices (may be NULL), and optionally the same slices of a target
+ * volume (scaled, FP32). */
+int ctlab_cnn_pack(const float *d_vol, int XN, int YN, int ZN, const int *d_z, int nb, float scale, void *d_in,
+                   float *d_center, float *d_target_of_vol, const float *d_vol_target, void *stream);
+
+/* Writes predicted slices (scaled) back into the volume: vol[y][x][z_b] = pred / scale. */
+int ctlab_cnn_unpack(const float *d_pred, int XN, int YN, int ZN, const int *d_z, int nb, float scale,
+                     float *d_vol, void *stream);
+
+/* MSE gradient 2 (pred - target) / n into channel 0 of a BF16 [n][16]
+ * tensor; d_acc (may be NULL) += sum of squared differences. */
+int ctlab_cnn_loss_grad(const float *d_pred, const float *d_target, long long n, void *d_g, double *d_acc,
+                        void *stream);
+
+/* Adam step (bias-corrected, step >= 1) on FP32 master parameters laid out
+ * as [co][9][ci] weights followed by co biases (d_w, moments d_m / d_v,
+ * gradient d_g, cleared afterwards); writes the BF16 weights d_wf
+ * [co][9][ci] and, if d_wt is not NULL, the flipped transposed copy
+ * d_wt [ci][9][co] (wt[ci][8 - tap][co] = w[co][tap][ci]). */
+int ctlab_cnn_adam(float *d_w, float *d_m, float *d_v, float *d_g, int co, int ci, float lr, float b1, float b2,
+                   float eps, int step, void *d_wf, void *d_wt, void *stream);
+
+/* ---------------------------------------------------------------------- */
 /* Phantoms (test and benchmark inputs)                                    */
 /* ---------------------------------------------------------------------- */
 
