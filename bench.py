@@ -46,9 +46,13 @@ def parse():
     ap.add_argument("--cpu-views", type=int, default=4, help="views in the bounded CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="dd3", choices=["dd3", "recon"],
+    ap.add_argument("--workload", default="dd3", choices=["dd3", "recon", "learned"],
                     help="dd3: the projector/backprojector throughput line (default); recon: OS-SART 24x30 and "
-                         "FISTA-TV 50 at 256x256x128 / 720 views with residual and RMSE per iteration")
+                         "FISTA-TV 50 at 256x256x128 / 720 views with residual and RMSE per iteration; learned: "
+                         "train the warm-start CNN on OS-SART 2- vs 30-iteration pairs, then time-to-residual "
+                         "learned vs plain")
+    ap.add_argument("--train-volumes", type=int, default=16, help="learned workload: training phantoms")
+    ap.add_argument("--train-steps", type=int, default=1500, help="learned workload: Adam steps")
     ap.add_argument("--recon-iters", type=int, default=0,
                     help="recon workload: iterations of each solver (0 = 30 OS-SART, 50 FISTA-TV); a smaller count "
                          "is a profiling case")
@@ -408,8 +412,9 @@ def run_recon(args):
         return res, rmse
 
     n_os, n_fi = (args.recon_iters, args.recon_iters) if args.recon_iters else (30, 50)
-    os_ms, _ = timed(lambda x, n: plan.os_sart(x, meas, os_num=24, iter_num=n_os))
-    fi_ms, _ = timed(lambda x, n: plan.fista_tv(x, meas, iter_num=n_fi, tv_lambda=1e-4))
+    with ClockSampler(local) as clk:
+        os_ms, _ = timed(lambda x, n: plan.os_sart(x, meas, os_num=24, iter_num=n_os))
+        fi_ms, _ = timed(lambda x, n: plan.fista_tv(x, meas, iter_num=n_fi, tv_lambda=1e-4))
     # per-iteration curves: OS-SART restarts nothing between iterations, so one
     # iteration per call is the same solve; FISTA's momentum is not resumable, so
     # its residuals come from one call and its RMSE only at the end
@@ -425,7 +430,121 @@ def run_recon(args):
                         "residual": [round(v, 6) for v in os_res], "rmse": [round(v, 7) for v in os_rmse]},
             "fista_tv": {"iterations": n_fi, "tv_lambda": 1e-4, "ms_total": fi_ms, "ms_per_iteration": fi_ms / n_fi,
                          "residual": [round(float(v), 6) for v in fi_res], "rmse_final": fi_rmse},
-            "phantom_rms": float(torch.sqrt(torch.mean(truth ** 2)))}
+            "phantom_rms": float(torch.sqrt(torch.mean(truth ** 2))), "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    plan.close()
+
+
+def run_learned(args):
+    """Learned warm start at 256x256x128 / 720 views / 384x128 detector, Poisson
+    noise I0 = 1e5.  Training pairs: for each seeded random-ellipsoid phantom, the
+    2-iteration and the 30-iteration OS-SART images (24 subsets) of its noisy
+    projections; 128 slice pairs per phantom.  The CNN trains with the library's own
+    kernels.  On a held-out phantom: plain = 30 OS-SART iterations from zero (residual
+    R30, device time T30); learned = 2 iterations + the CNN + the fewest further
+    iterations whose residual reaches R30.  Times are CUDA-event device times of the
+    solver calls; residual evaluations happen in separate, untimed passes."""
+    import torch
+
+    import ctlab_b200 as cb
+    from ctlab_b200 import geometry as G
+    from ctlab_b200.learned import WarmStartNet
+
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    g = G.config3()
+    hx, hy, hz = G.half_extents(g)
+    plan = cb.Plan(g, device=local)
+    stream = torch.cuda.current_stream()
+    OS, IT, I0, SCALE = 24, 30, 1e5, 1.0 / 0.03
+
+    def event_ms(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    def scan(seed):
+        truth = torch.zeros(g.vol_shape, dtype=torch.float32, device="cuda")
+        cb.ellipsoid_phantom(truth, g, cb.random_ellipsoids(seed, hx, hy, hz))
+        clean = torch.zeros(g.prj_shape, dtype=torch.float32, device="cuda")
+        plan.proj(truth, clean)
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(seed)
+        counts = torch.poisson(I0 * torch.exp(-clean), generator=gen)
+        return truth, -torch.log(torch.clamp(counts, min=1.0) / I0)
+
+    t0 = time.perf_counter()
+    pairs = []
+    for s in range(args.train_volumes):
+        _, meas = scan(1000 + s)
+        x = torch.zeros(g.vol_shape, dtype=torch.float32, device="cuda")
+        plan.os_sart(x, meas, os_num=OS, iter_num=2)
+        x2 = x.clone()
+        plan.os_sart(x, meas, os_num=OS, iter_num=IT - 2)
+        pairs.append((x2, x))
+        del meas
+    torch.cuda.synchronize()
+    t_data = time.perf_counter() - t0
+
+    net = WarmStartNet(seed=0)
+    rng = np.random.default_rng(0)
+    losses = []
+    t0 = time.perf_counter()
+    for step in range(args.train_steps):
+        lr = 1e-3 * 0.5 * (1 + np.cos(np.pi * step / args.train_steps))
+        x2, x30 = pairs[int(rng.integers(len(pairs)))]
+        losses.append(net.train_step(x2, x30, rng.integers(0, g.ZN, 8), SCALE, lr=max(lr, 2e-5)))
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+
+    truth, meas = scan(7)
+    clk = ClockSampler(local).__enter__()
+    # plain: 30 iterations from zero
+    x = torch.zeros_like(truth)
+    t30 = event_ms(lambda: plan.os_sart(x, meas, os_num=OS, iter_num=IT))
+    xr = torch.zeros_like(truth)
+    res_plain = plan.os_sart(xr, meas, os_num=OS, iter_num=IT, residuals=True)
+    r30 = float(res_plain[-1])
+    rmse_plain = float(torch.sqrt(torch.mean((x - truth) ** 2)))
+    # learned: 2 iterations, the network, then iterations until the residual reaches R30
+    xl = torch.zeros_like(truth)
+    t2 = event_ms(lambda: plan.os_sart(xl, meas, os_num=OS, iter_num=2))
+    xw = torch.zeros_like(truth)
+    tcnn = event_ms(lambda: net.predict_volume(xl, SCALE, xw))
+    rmse_warm = float(torch.sqrt(torch.mean((xw - truth) ** 2)))
+    xc = xw.clone()
+    res_cont = plan.os_sart(xc, meas, os_num=OS, iter_num=IT, residuals=True)
+    hits = [k + 1 for k, r in enumerate(res_cont) if r <= r30]
+    k = hits[0] if hits else None
+    tk = 0.0
+    xk = xw.clone()
+    if k:
+        tk = event_ms(lambda: plan.os_sart(xk, meas, os_num=OS, iter_num=k))
+    rmse_learned = float(torch.sqrt(torch.mean((xk - truth) ** 2)))
+    clk.__exit__(None, None, None)
+    x2_only = torch.zeros_like(truth)
+    plan.os_sart(x2_only, meas, os_num=OS, iter_num=2)
+    rmse_2 = float(torch.sqrt(torch.mean((x2_only - truth) ** 2)))
+    t_learned = t2 + tcnn + tk
+    line = {"metric": "learned warm start: time to the plain 30-iteration OS-SART residual",
+            "workload": "learned_warm_start_256x256x128_720v_384x128", "n_gpus": 1,
+            "data": "synthetic (seeded random-ellipsoid phantoms, Poisson noise I0=1e5)",
+            "network": "2.5D residual CNN, 5 slices in, 8 conv3x3 layers of 64 channels, BF16 weights / FP32 accumulate",
+            "training": {"volumes": args.train_volumes, "slice_pairs": args.train_volumes * g.ZN,
+                         "steps": args.train_steps, "batch_slices": 8, "data_s": t_data, "train_s": t_train,
+                         "loss_first": float(np.mean(losses[:20])), "loss_last": float(np.mean(losses[-20:]))},
+            "plain": {"iterations": IT, "ms": t30, "residual": r30, "rmse": rmse_plain},
+            "learned": {"os_sart_2_ms": t2, "cnn_ms": tcnn, "continued_iterations": k, "continued_ms": tk,
+                        "ms": t_learned if k else None, "residual_after_cnn": float(res_cont[0]),
+                        "rmse_2_iterations": rmse_2, "rmse_after_cnn": rmse_warm, "rmse": rmse_learned},
+            "time_ratio": (t_learned / t30) if k else None, "target_ratio": 0.5,
+            "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
     plan.close()
 
@@ -434,6 +553,8 @@ def main():
     args = parse()
     if args.workload == "recon":
         run_recon(args)
+    elif args.workload == "learned":
+        run_learned(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
