@@ -91,6 +91,11 @@ _SIGNATURES = {
     "ctlab_fista_tv": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_float, C.c_float, C.c_float,
                                  C.c_float, _fp, _vp]),
     "ctlab_cg": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int, _fp, _vp]),
+    "ctlab_plan_autotune": (C.c_int, [_vp, _vp, _vp, C.c_char_p, _fp]),
+    "ctlab_batch_create": (C.c_int, [C.POINTER(_vp), C.c_int, C.POINTER(_vp)]),
+    "ctlab_batch_destroy": (C.c_int, [_vp]),
+    "ctlab_batch_voxel_views": (C.c_longlong, [_vp]),
+    "ctlab_batch_proj": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp), C.c_int, _vp]),
     "ctlab_cnn_conv": (C.c_int, [_vp, C.c_int, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp,
                                  _vp, _vp, _vp]),
     "ctlab_cnn_wgrad": (C.c_int, [_vp, C.c_int, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp]),

@@ -234,8 +234,20 @@ struct ProjTStaging {
     bool ok = false;
 };
 // gcap limits the views per CTA (launches whose views group one by one use
-// a staging planned with gcap = 1).
-ProjTStaging proj_t_staging(const HostGeometry &g, int gcap = 16);
+// a staging planned with gcap = 1); nstage > 0 fixes the stage depth.
+ProjTStaging proj_t_staging(const HostGeometry &g, int gcap = 16, int nstage = 0);
+size_t proj_t_smem_bytes(const ProjTStaging &st);
+
+// One scan of a batched (persistent) projector launch: its arguments and TMA
+// maps, in device memory.
+struct __align__(64) ProjBatchCase {
+    CUtensorMap tm_y, tm_x;
+    ProjArgs a;
+};
+// Runs work items (case, detector tile, view group, row block) of the cases
+// on a persistent grid; *d_counter must be 0 (stream-ordered).
+cudaError_t launch_proj_t_batch(const ProjBatchCase *d_cases, const int4 *d_items, int nitems, int *d_counter,
+                                size_t smem, int grid, cudaStream_t s);
 ProjGroups proj_t_make_groups(const HostGeometry &g, const std::vector<int> &list, const ProjTStaging &st);
 cudaError_t launch_proj_t(const ProjArgs &a, const ProjTStaging &st, const CUtensorMap &tmy, const CUtensorMap &tmx,
                           cudaStream_t s, int *launches);

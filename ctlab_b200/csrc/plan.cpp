@@ -292,6 +292,13 @@ int plan_check_device_error(ctlab_plan *p, cudaStream_t s)
     return CTLAB_OK;
 }
 
+int plan_encode_zt(ctlab_plan *p, int orientation, const ProjTStaging &st, CUtensorMap *out)
+{
+    const HostGeometry &g = p->g;
+    return orientation == 0 ? encode_zt_map(out, p->d_zt_y, g.XN, g.ZN, g.YN, p->zt_rs_y, st.CB, st.KB)
+                            : encode_zt_map(out, p->d_zt_x, g.YN, g.ZN, g.XN, p->zt_rs_x, st.CB, st.KB);
+}
+
 void timing_mark(ctlab_plan *p, int which, cudaStream_t s)
 {
     if (p->timing) cudaEventRecord(p->ev[which], s);

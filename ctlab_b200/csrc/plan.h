@@ -68,5 +68,7 @@ int plan_back_list(ctlab_plan *p, const int *d_list, int n, const unsigned char 
 int plan_upload_list(ctlab_plan *p, const int *h_views, int n, cudaStream_t s);
 int plan_check_device_error(ctlab_plan *p, cudaStream_t s);
 void timing_mark(ctlab_plan *p, int which, cudaStream_t s);
+// TMA map of the plan's z-prefix array of one orientation for a staging.
+int plan_encode_zt(ctlab_plan *p, int orientation, const ProjTStaging &st, CUtensorMap *out);
 
 } // namespace ctlab

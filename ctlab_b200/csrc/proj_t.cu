@@ -84,33 +84,52 @@ __device__ __forceinline__ float4 lds_f32x4(uint32_t addr)
     return v;
 }
 
+// Shared state of one projector tile besides the stage ring.
+struct ProjTShm {
+    uint64_t full[kTMaxStage], empty[kTMaxStage];
+    TSlice info[kTMaxStage];
+    double c0[kTMaxG][kTU + 1], m[kTMaxG][kTU + 1], r[kTMaxG][kTU];
+    double ga0[kTMaxG], rmin[kTMaxG], rmax[kTMaxG];
+    float Z0[kTMaxG], emin[kTMaxG], emax[kTMaxG];
+    int pos_list[kTMaxG];
+    int abort;
+    double red[kTMaxCWarps + 1];
+};
+
+// One CTA's work: detector tile bx (32 columns), view group by, row block bz
+// of the launch described by a.  smem: the 128-byte aligned dynamic shared
+// memory (stages and z-boundary tables).
 template <int NR>
-__global__ void __launch_bounds__(kTMaxThreads, 1)
-    dd3_proj_t_kernel(ProjArgs a, const __grid_constant__ CUtensorMap tm_y, const __grid_constant__ CUtensorMap tm_x)
+__device__ __forceinline__ void proj_t_tile(const ProjArgs &a, const CUtensorMap *tm_y_p, const CUtensorMap *tm_x_p,
+                                            int bx, int by, int bz, unsigned char *smem, ProjTShm &sh)
 {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    // TMA destinations need 128-byte alignment (the launch adds 128 bytes)
-    unsigned char *smem = smem_raw + ((128 - (smem_addr(smem_raw) & 127)) & 127);
     const int G = a.G, RB = a.t_rb, NWC = G * RB;
-    const int vbase = blockIdx.z * RB * NR; // first detector row of this CTA (rows split over grid z)
+    const int vbase = bz * RB * NR; // first detector row of this CTA (rows split over CTAs)
     const int nstage = a.t_nstage;
     const int CB = a.t_cb, KB = a.t_kb, KR = a.t_kr, EP = a.t_ep, GT = a.t_gtab;
     const int stage_floats = KR * CB;
-    float *stage0 = reinterpret_cast<float *>(smem);                    // [nstage][KR][CB]
+    float *stage0 = reinterpret_cast<float *>(smem);                          // [nstage][KR][CB]
     float *s_e = reinterpret_cast<float *>(smem + 4 * stage_floats * nstage); // [GT][EP]
-    __shared__ __align__(8) uint64_t s_full[kTMaxStage], s_empty[kTMaxStage];
-    __shared__ TSlice s_info[kTMaxStage];
-    __shared__ double s_c0[kTMaxG][kTU + 1], s_m[kTMaxG][kTU + 1], s_r[kTMaxG][kTU];
-    __shared__ double s_ga0[kTMaxG], s_rmin[kTMaxG], s_rmax[kTMaxG];
-    __shared__ float s_Z0[kTMaxG], s_emin[kTMaxG], s_emax[kTMaxG];
-    __shared__ int s_pos_list[kTMaxG];
-    __shared__ int s_abort;
-    __shared__ double s_red[kTMaxCWarps + 1];
+    auto &s_full = sh.full;
+    auto &s_empty = sh.empty;
+    auto &s_info = sh.info;
+    auto &s_c0 = sh.c0;
+    auto &s_m = sh.m;
+    auto &s_r = sh.r;
+    auto &s_ga0 = sh.ga0;
+    auto &s_rmin = sh.rmin;
+    auto &s_rmax = sh.rmax;
+    auto &s_Z0 = sh.Z0;
+    auto &s_emin = sh.emin;
+    auto &s_emax = sh.emax;
+    auto &s_pos_list = sh.pos_list;
+    auto &s_abort = sh.abort;
+    auto &s_red = sh.red;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid < G) s_pos_list[tid] = a.groups[blockIdx.y * G + tid];
+    if (tid < G) s_pos_list[tid] = a.groups[by * G + tid];
     if (tid == 0) s_abort = 0;
-    const int u0 = blockIdx.x * kTU;
+    const int u0 = bx * kTU;
     const int nu = min(kTU, a.DNU - u0);
     const DetTable t = det_table_layout(a.DNU, a.DNV);
     const double *det = a.det;
@@ -190,7 +209,7 @@ __global__ void __launch_bounds__(kTMaxThreads, 1)
     double r2 = 0.0;
     if (warp == NWC) {
         // ------------------------------ producer ------------------------------
-        const CUtensorMap *tm = xdrv ? &tm_x : &tm_y;
+        const CUtensorMap *tm = xdrv ? tm_x_p : tm_y_p;
         const int uq = min(lane, nu - 1);
         int issued = 0;
         for (int j = 0; j < na; ++j) {
@@ -447,6 +466,63 @@ __global__ void __launch_bounds__(kTMaxThreads, 1)
     }
 }
 
+__device__ __forceinline__ unsigned char *align128(unsigned char *p)
+{
+    return p + ((128 - (smem_addr(p) & 127)) & 127);
+}
+
+template <int NR>
+__global__ void __launch_bounds__(kTMaxThreads, 1)
+    dd3_proj_t_kernel(ProjArgs a, const __grid_constant__ CUtensorMap tm_y, const __grid_constant__ CUtensorMap tm_x)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ ProjTShm sh;
+    // TMA destinations need 128-byte alignment (the launch adds 128 bytes)
+    proj_t_tile<NR>(a, &tm_y, &tm_x, blockIdx.x, blockIdx.y, blockIdx.z, align128(smem_raw), sh);
+}
+
+// Persistent projector over many scans: CTAs take (case, tile, group, row
+// block) work items from a queue (items sorted longest first) and run them
+// with each case's arguments and TMA maps from global memory.
+__global__ void __launch_bounds__(kTMaxThreads, 1)
+    dd3_proj_t_batch_kernel(const ProjBatchCase *__restrict__ cases, const int4 *__restrict__ items, int nitems,
+                            int *counter)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ ProjTShm sh;
+    __shared__ ProjArgs s_a;
+    __shared__ int s_item;
+    unsigned char *smem = align128(smem_raw);
+    const int tid = threadIdx.x;
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= nitems) break;
+        const int4 w = items[it];
+        const ProjBatchCase &c = cases[w.x];
+        {
+            const int *src = reinterpret_cast<const int *>(&c.a);
+            int *dst = reinterpret_cast<int *>(&s_a);
+            for (int i = tid; i < (int)(sizeof(ProjArgs) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+        }
+        __syncthreads();
+        switch (s_a.t_nr) {
+        case 4: proj_t_tile<4>(s_a, &c.tm_y, &c.tm_x, w.y, w.z, w.w, smem, sh); break;
+        case 8: proj_t_tile<8>(s_a, &c.tm_y, &c.tm_x, w.y, w.z, w.w, smem, sh); break;
+        case 16: proj_t_tile<16>(s_a, &c.tm_y, &c.tm_x, w.y, w.z, w.w, smem, sh); break;
+        default: proj_t_tile<32>(s_a, &c.tm_y, &c.tm_x, w.y, w.z, w.w, smem, sh); break;
+        }
+        // every warp is done with this item's barriers and buffers
+        __syncthreads();
+        if (tid < kTMaxStage) {
+            asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(&sh.full[tid])) : "memory");
+            asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(&sh.empty[tid])) : "memory");
+        }
+        __syncthreads();
+    }
+}
+
 size_t smem_bytes(const ProjTStaging &st)
 {
     return 128 + 4 * (size_t)st.KR * st.CB * st.nstage + sizeof(float) * (size_t)st.G * st.EP;
@@ -581,7 +657,20 @@ int env_int(const char *name, int dflt)
 
 } // namespace
 
-ProjTStaging proj_t_staging(const HostGeometry &g, int gcap)
+size_t proj_t_smem_bytes(const ProjTStaging &st) { return smem_bytes(st); }
+
+cudaError_t launch_proj_t_batch(const ProjBatchCase *d_cases, const int4 *d_items, int nitems, int *d_counter,
+                                size_t smem, int grid, cudaStream_t s)
+{
+    if (nitems <= 0) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(dd3_proj_t_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    dd3_proj_t_batch_kernel<<<grid, kTMaxThreads, smem, s>>>(d_cases, d_items, nitems, d_counter);
+    return cudaGetLastError();
+}
+
+ProjTStaging proj_t_staging(const HostGeometry &g, int gcap, int nstage_fix)
 {
     ProjTStaging st;
     st.ok = false;
@@ -590,7 +679,7 @@ ProjTStaging proj_t_staging(const HostGeometry &g, int gcap)
     // CTLAB_PROJT_CBMAX caps the staged columns
     const int gmax = std::max(1, std::min(std::min(env_int("CTLAB_PROJT_GMAX", 8), kTMaxG), gcap));
     const int want_zs = env_int("CTLAB_PROJT_ZS", 0);
-    const int want_stage = env_int("CTLAB_PROJT_NSTAGE", 0);
+    const int want_stage = nstage_fix > 0 ? nstage_fix : env_int("CTLAB_PROJT_NSTAGE", 0);
     const int cbmax = std::min(env_int("CTLAB_PROJT_CBMAX", 256), 256);
     std::vector<int> all(g.PN);
     for (int i = 0; i < g.PN; ++i) all[i] = i;

@@ -146,6 +146,14 @@ class Plan:
     def last_launches(self) -> int:
         return int(self.lib.ctlab_plan_last_launches(self.handle))
 
+    def autotune(self, vol, out, cache_path: str | None = None) -> float:
+        """Picks the fastest projector staging for this scan (ctlab_plan_autotune);
+        returns its time in ms, or -1 when it came from the cache."""
+        ms = C.c_float()
+        check(self.lib.ctlab_plan_autotune(self.handle, self._p(vol), self._p(out),
+                                           None if cache_path is None else cache_path.encode(), C.byref(ms)))
+        return ms.value
+
     def proj(self, vol, out, mask=None, stream=None):
         check(self.lib.ctlab_proj(self.handle, self._p(vol), self._p(mask), self._p(out), self._stream(stream)))
         return out
@@ -225,3 +233,39 @@ def random_ellipsoids(seed: int, half_x: float, half_y: float, half_z: float, n_
     if n < 0:
         check(-n)
     return buf[:n].copy()
+
+
+class Batch:
+    """Projects the scans of several z-prefix plans with one persistent launch
+    (ctlab_batch_*), optionally replayed from a CUDA graph."""
+
+    def __init__(self, plans):
+        self.lib = load()
+        self.plans = list(plans)
+        arr = (C.c_void_p * len(self.plans))(*[p.handle for p in self.plans])
+        h = C.c_void_p()
+        check(self.lib.ctlab_batch_create(arr, len(self.plans), C.byref(h)))
+        self.handle = h
+
+    @property
+    def voxel_views(self) -> int:
+        return int(self.lib.ctlab_batch_voxel_views(self.handle))
+
+    def proj(self, vols, outs, masks=None, graph: bool = False, stream=None):
+        n = len(self.plans)
+        V = (C.c_void_p * n)(*[v.data_ptr() for v in vols])
+        O = (C.c_void_p * n)(*[o.data_ptr() for o in outs])
+        M = None if masks is None else (C.c_void_p * n)(*[None if m is None else m.data_ptr() for m in masks])
+        check(self.lib.ctlab_batch_proj(self.handle, V, M, O, 1 if graph else 0, Plan._stream(stream)))
+        return outs
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.ctlab_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -119,6 +119,26 @@ def config3() -> DD3Geometry:
                             XN=256, YN=256, ZN=128, dx=0.5, dz=0.5)
 
 
+def config4(seed: int = 7, n: int = 48) -> list[DD3Geometry]:
+    """The uneven batch: n scans with volumes from {128^3, 192x192x96, 256x256x64,
+    384x384x32} (1 mm voxels), 180-720 views, detectors 256-768 cells wide and 32-64
+    rows; cell sizes chosen so the detector covers the volume (10 % margin)."""
+    rng = np.random.default_rng(seed)
+    vols = [(128, 128, 128), (192, 192, 96), (256, 256, 64), (384, 384, 32)]
+    out = []
+    for _ in range(n):
+        XN, YN, ZN = vols[int(rng.integers(len(vols)))]
+        PN = int(rng.integers(180, 721))
+        DNU = int(rng.integers(256, 769))
+        DNV = int(rng.integers(32, 65))
+        mag = SDD / SOD
+        col = 1.1 * XN * math.sqrt(2.0) * mag / DNU
+        row = 1.1 * ZN * mag / DNV
+        out.append(DD3Geometry.flat(sid=SOD, sdd=SDD, DNU=DNU, DNV=DNV, col_size=col, row_size=row, PN=PN,
+                                    XN=XN, YN=YN, ZN=ZN, dx=1.0, dz=1.0))
+    return out
+
+
 def small(PN: int = 24, XN: int = 24, YN: int = 20, ZN: int = 12, DNU: int = 40, DNV: int = 14,
           dx: float = 0.5, dz: float = 0.5, col_size: float = 0.9, row_size: float = 0.8,
           col_offset: float = 0.0, row_offset: float = 0.0, start: float = 0.0,

@@ -243,6 +243,35 @@ int ctlab_sart_back_weight(float *d_vol, float *d_recon, const float *d_col_sum,
                            void *stream);
 
 /* ---------------------------------------------------------------------- */
+/* Batched projection of many scans and the projector autotuner (no       */
+/* counterpart in the reference)                                          */
+/* ---------------------------------------------------------------------- */
+
+/* Times the z-prefix projector of `plan` under each candidate staging (views
+ * per CTA 2..16, stage depth 2..4) on d_vol (d_prj receives projections),
+ * keeps the fastest, and appends it to the JSON-lines cache file cache_path
+ * (may be NULL) keyed by the scan geometry; a cached scan is not re-timed
+ * (*best_ms = -1).  Synchronous. */
+int ctlab_plan_autotune(ctlab_plan *plan, const float *d_vol, float *d_prj, const char *cache_path,
+                        float *best_ms);
+
+/* A batch projects the scans of n z-prefix plans (one device) together. */
+typedef struct ctlab_batch ctlab_batch;
+int ctlab_batch_create(ctlab_plan *const *plans, int n, ctlab_batch **out);
+int ctlab_batch_destroy(ctlab_batch *batch);
+/* Sum over the cases of XN*YN*ZN*PN. */
+long long ctlab_batch_voxel_views(const ctlab_batch *batch);
+/* Projects d_vols[i] (masks d_masks[i], d_masks may be NULL) into d_prjs[i]
+ * for every case: each case's z-prefixes, then one persistent projector
+ * launch over the work items of all cases (sorted longest first).  With
+ * use_graph the sequence is captured into a CUDA graph on the first call
+ * (stream must not be the legacy default stream) and replayed while the
+ * volume and mask pointers stay the same.  Waits for the stream's previous
+ * work before it rewrites its case table. */
+int ctlab_batch_proj(ctlab_batch *batch, const float *const *d_vols, const unsigned char *const *d_masks,
+                     float *const *d_prjs, int use_graph, void *stream);
+
+/* ---------------------------------------------------------------------- */
 /* Learned warm start: 2.5D residual CNN kernels (no counterpart in the   */
 /* reference; the network that warm-starts OS-SART)                       */
 /* ---------------------------------------------------------------------- */
