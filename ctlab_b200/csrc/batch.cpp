@@ -2,20 +2,25 @@
 // autotuner.
 //
 // A batch holds plans of different geometries.  One run builds every
-// case's slice-major z-prefixes, then projects all cases with ONE
-// persistent launch: CTAs take (case, detector tile, view group, row block)
-// work items from a queue sorted longest first, so cases of uneven size
-// share the GPU instead of running one after another.  With use_graph the
-// whole run is captured once into a CUDA graph and replayed.
+// case's slice-major z-prefixes, then projects all cases with persistent
+// launches: CTAs take (case, detector tile, view group, row block) work
+// items from a queue sorted longest first, so cases of uneven size share the
+// GPU instead of running one after another.  Cases whose projector has the
+// same rows per consumer warp share one launch (its kernel is compiled for
+// that row count; the cases' arguments and TMA maps travel as its kernel
+// parameters); launches of different row counts run on forked streams, each
+// filling the SMs the others free.  With use_graph the whole run is captured
+// once into a CUDA graph and replayed.
 //
 // The autotuner times the projector of a plan under each candidate staging
-// (views per CTA, stage depth), keeps the fastest and records it in a JSON
-// cache keyed by the scan geometry, so later plans of the same scan skip
-// the timing.
+// (views per CTA, detector-row split, stage depth), keeps the fastest and
+// records it in a JSON cache keyed by the scan geometry, so later plans of
+// the same scan skip the timing.
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <sstream>
@@ -26,15 +31,29 @@
 
 using namespace ctlab;
 
+// Cases whose launches share the rows per consumer warp run in one
+// persistent launch (up to kProjBatchMaxCases cases each, their arguments in
+// the kernel parameters); launches of different row counts run side by side.
+struct BatchLaunch {
+    int nr = 0;             // detector rows per consumer warp
+    std::vector<int> cases; // plan indices; work items name positions here
+    int first = 0;          // first work item (d_items)
+    int count = 0;          // work items
+    size_t smem = 0;
+    double cost = 0.0;
+    std::unique_ptr<ProjBatchParams> params;
+};
+
 struct ctlab_batch {
     int device = 0;
     std::vector<ctlab_plan *> plans;
-    ProjBatchCase *h_cases = nullptr; // pinned: graph replays copy from it
-    ProjBatchCase *d_cases = nullptr;
     int4 *d_items = nullptr;
     int nitems = 0;
-    int *d_counter = nullptr;
-    size_t smem = 0;
+    int *d_counter = nullptr; // one queue counter per launch
+    std::vector<BatchLaunch> launches;
+    std::vector<cudaStream_t> side; // launches after the first
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
     int grid = 0;
     cudaGraphExec_t gexec = nullptr;
     std::vector<const void *> graph_ptrs; // buffers the graph was captured with
@@ -69,11 +88,8 @@ void fill_case(ctlab_plan *p, float *d_prj, ProjBatchCase &c)
     a.zt_rs_y = p->zt_rs_y; a.zt_rs_x = p->zt_rs_x;
     a.t_cb = st.CB; a.t_kb = st.KB; a.t_kr = st.KR;
     a.t_nstage = st.nstage; a.t_ep = st.EP; a.t_gtab = st.G;
-    int nr = st.NR, rb = st.RB;
-    while (a.G * rb * 2 <= 16 && nr >= 16) {
-        nr /= 2;
-        rb *= 2;
-    }
+    int nr, rb;
+    proj_t_split(st, a.G, nr, rb);
     a.t_rb = rb; a.t_nr = nr; a.t_zs = st.ZS;
     c.tm_y = p->tm_y;
     c.tm_x = p->tm_x;
@@ -102,7 +118,7 @@ unsigned long long scan_key(const HostGeometry &g)
 
 std::mutex g_cache_mu;
 
-bool cache_lookup(const char *path, unsigned long long key, int &gcap, int &nstage)
+bool cache_lookup(const char *path, unsigned long long key, int &gcap, int &nstage, int &zs)
 {
     if (!path) return false;
     std::lock_guard<std::mutex> lk(g_cache_mu);
@@ -118,20 +134,23 @@ bool cache_lookup(const char *path, unsigned long long key, int &gcap, int &nsta
         if (std::sscanf(line.c_str() + pa + 7, "%d", &a) == 1 && std::sscanf(line.c_str() + pb + 9, "%d", &b) == 1) {
             gcap = a;
             nstage = b;
+            zs = 0;
+            const size_t pz = line.find("\"zs\":");
+            if (pz != std::string::npos && std::sscanf(line.c_str() + pz + 5, "%d", &a) == 1) zs = a;
             return true;
         }
     }
     return false;
 }
 
-void cache_store(const char *path, unsigned long long key, int gcap, int nstage, float ms)
+void cache_store(const char *path, unsigned long long key, int gcap, int nstage, int zs, float ms)
 {
     if (!path) return;
     std::lock_guard<std::mutex> lk(g_cache_mu);
     std::ofstream f(path, std::ios::app);
-    char buf[160];
-    std::snprintf(buf, sizeof buf, "{\"scan\": \"%016llx\", \"gcap\": %d, \"nstage\": %d, \"ms\": %.4f}\n", key, gcap,
-                  nstage, ms);
+    char buf[192];
+    std::snprintf(buf, sizeof buf, "{\"scan\": \"%016llx\", \"gcap\": %d, \"nstage\": %d, \"zs\": %d, \"ms\": %.4f}\n",
+                  key, gcap, nstage, zs, ms);
     f << buf;
 }
 
@@ -170,9 +189,9 @@ int ctlab_plan_autotune(ctlab_plan *plan, const float *d_vol, float *d_prj, cons
     DeviceGuard dg(plan->device);
     const HostGeometry &g = plan->g;
     const unsigned long long key = scan_key(g);
-    int gcap = 0, ns = 0;
-    if (cache_lookup(cache_path, key, gcap, ns)) {
-        ProjTStaging st = proj_t_staging(g, gcap, ns);
+    int gcap = 0, ns = 0, zs = 0;
+    if (cache_lookup(cache_path, key, gcap, ns, zs)) {
+        ProjTStaging st = proj_t_staging(g, gcap, ns, zs);
         if (st.ok) {
             int rc = apply_staging(plan, st);
             if (rc != CTLAB_OK) return rc;
@@ -185,13 +204,17 @@ int ctlab_plan_autotune(ctlab_plan *plan, const float *d_vol, float *d_prj, cons
     CTLAB_CUDA_TRY(cudaEventCreate(&e1));
     float best = 1e30f;
     ProjTStaging best_st = plan->tst;
-    int best_g = 16, best_n = 0;
-    std::vector<std::pair<int, int>> seen;
-    for (int gc : {16, 8, 4, 2}) {
-        for (int n : {2, 3, 4}) {
-            ProjTStaging st = proj_t_staging(g, gc, n);
-            if (!st.ok || st.nstage != n) continue;
-            const std::pair<int, int> sig{st.G * 10 + st.nstage, st.ZS * 1000 + st.CB};
+    int best_g = 16, best_n = 0, best_z = 0;
+    std::vector<std::vector<int>> seen;
+    // candidates: views per CTA capped at 16 / 8 / 4 / 2, detector rows split
+    // over 1 / 2 / 4 CTAs (the deepest stage ring that fits); each distinct
+    // staging timed once
+    for (int gc : {16, 8, 4, 2})
+        for (int z : {1, 2, 4}) {
+            ProjTStaging st = proj_t_staging(g, gc, 0, z);
+            const int n = st.nstage;
+            if (!st.ok) continue;
+            const std::vector<int> sig{st.G, st.NR, st.RB, st.ZS, st.CB, st.KB, st.nstage};
             if (std::find(seen.begin(), seen.end(), sig) != seen.end()) continue;
             seen.push_back(sig);
             int rc = apply_staging(plan, st);
@@ -211,15 +234,32 @@ int ctlab_plan_autotune(ctlab_plan *plan, const float *d_vol, float *d_prj, cons
                 best_st = st;
                 best_g = gc;
                 best_n = n;
+                best_z = z;
             }
         }
-    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     int rc = apply_staging(plan, best_st);
     if (rc != CTLAB_OK) return rc;
-    cache_store(cache_path, key, best_g, best_n, best);
+    cache_store(cache_path, key, best_g, best_n, best_z, best);
     if (best_ms) *best_ms = best;
+    return set_status(CTLAB_OK, "");
+}
+
+int ctlab_plan_proj_tiles(const ctlab_plan *plan, int *tiles)
+{
+    if (!plan || !tiles) return set_status(CTLAB_ERR_INVALID_ARG, "null plan or output");
+    if (plan->sat_mode != CTLAB_SAT_ZPREFIX)
+        return set_status(CTLAB_ERR_UNSUPPORTED, "projector tiles are defined for sat mode ZPREFIX");
+    const ProjTStaging &st = plan->tst;
+    tiles[0] = st.G;
+    tiles[1] = st.NR;
+    tiles[2] = st.RB;
+    tiles[3] = st.ZS;
+    tiles[4] = st.CB;
+    tiles[5] = st.KB;
+    tiles[6] = st.nstage;
+    tiles[7] = (plan->g.DNU + 31) / 32 * plan->groups_all_n * st.ZS;
     return set_status(CTLAB_OK, "");
 }
 
@@ -238,40 +278,79 @@ int ctlab_batch_create(ctlab_plan *const *plans, int n, ctlab_batch **out)
     b->device = dev;
     b->plans.assign(plans, plans + n);
     DeviceGuard dg(dev);
-    // work items, longest first: per item the slices of the driving axis times
-    // the views of its group times the detector rows of its block
-    struct Item {
-        int4 w;
-        double cost;
-    };
-    std::vector<Item> items;
+    // work items: per item the slices of the driving axis times the views of
+    // its group times the detector rows of its block.  Cases go to launches
+    // by rows per warp (in chunks of kProjBatchMaxCases); items longest first
+    // within a launch, the launch with the most work first.
+    std::vector<std::vector<int4>> case_items(n);
+    std::vector<std::vector<double>> case_cost(n);
     for (int i = 0; i < n; ++i) {
         ctlab_plan *p = plans[i];
         ProjBatchCase c;
         fill_case(p, nullptr, c);
-        b->smem = std::max(b->smem, proj_t_smem_bytes(p->tst));
         const int tiles = (p->g.DNU + 31) / 32;
         const int rows = c.a.t_nr * c.a.t_rb;
+        const int na = std::max(p->g.XN, p->g.YN);
         for (int gy = 0; gy < c.a.ngroups; ++gy)
             for (int bx = 0; bx < tiles; ++bx)
                 for (int bz = 0; bz < c.a.t_zs; ++bz) {
-                    const int na = std::max(p->g.XN, p->g.YN);
-                    items.push_back({make_int4(i, bx, gy, bz), (double)na * c.a.G * std::min(rows, p->g.DNV - bz * rows)});
+                    case_items[i].push_back(make_int4(0, bx, gy, bz));
+                    case_cost[i].push_back((double)na * c.a.G * std::min(rows, p->g.DNV - bz * rows));
                 }
+        BatchLaunch *L = nullptr;
+        for (BatchLaunch &l : b->launches)
+            if (l.nr == c.a.t_nr && (int)l.cases.size() < kProjBatchMaxCases) L = &l;
+        if (!L) {
+            b->launches.emplace_back();
+            L = &b->launches.back();
+            L->nr = c.a.t_nr;
+        }
+        L->cases.push_back(i);
+        L->smem = std::max(L->smem, proj_t_smem_bytes(p->tst));
+        for (double x : case_cost[i]) L->cost += x;
         b->voxel_views += (long long)p->g.XN * p->g.YN * p->g.ZN * p->g.PN;
     }
-    std::stable_sort(items.begin(), items.end(), [](const Item &x, const Item &y) { return x.cost > y.cost; });
-    std::vector<int4> w(items.size());
-    for (size_t k = 0; k < items.size(); ++k) w[k] = items[k].w;
+    std::stable_sort(b->launches.begin(), b->launches.end(),
+                     [](const BatchLaunch &x, const BatchLaunch &y) { return x.cost > y.cost; });
+    std::vector<int4> w;
+    for (BatchLaunch &l : b->launches) {
+        std::vector<std::pair<double, int4>> mine;
+        for (int k = 0; k < (int)l.cases.size(); ++k) {
+            const int i = l.cases[k];
+            for (size_t q = 0; q < case_items[i].size(); ++q) {
+                int4 it = case_items[i][q];
+                it.x = k;
+                mine.push_back({case_cost[i][q], it});
+            }
+        }
+        std::stable_sort(mine.begin(), mine.end(),
+                         [](const std::pair<double, int4> &x, const std::pair<double, int4> &y) { return x.first > y.first; });
+        l.first = (int)w.size();
+        l.count = (int)mine.size();
+        for (const auto &m : mine) w.push_back(m.second);
+        l.params.reset(new (std::nothrow) ProjBatchParams());
+        if (!l.params) {
+            ctlab_batch_destroy(b);
+            return set_status(CTLAB_ERR_OOM, "host allocation failed");
+        }
+    }
     b->nitems = (int)w.size();
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     b->grid = sms;
-    cudaError_t e = cudaMalloc(&b->d_cases, sizeof(ProjBatchCase) * n);
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_items, sizeof(int4) * w.size());
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_counter, sizeof(int));
-    if (e == cudaSuccess) e = cudaMallocHost(&b->h_cases, sizeof(ProjBatchCase) * n);
+    const int nl = (int)b->launches.size();
+    cudaError_t e = cudaMalloc(&b->d_items, sizeof(int4) * w.size());
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_counter, sizeof(int) * nl);
     if (e == cudaSuccess) e = cudaMemcpy(b->d_items, w.data(), sizeof(int4) * w.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && nl > 1) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+    for (int k = 1; k < nl && e == cudaSuccess; ++k) {
+        cudaStream_t st = nullptr;
+        cudaEvent_t ev = nullptr;
+        e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+        if (e == cudaSuccess) b->side.push_back(st);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (e == cudaSuccess) b->join.push_back(ev);
+    }
     if (e != cudaSuccess) {
         ctlab_batch_destroy(b);
         return cuda_status(e, "batch buffers");
@@ -285,10 +364,11 @@ int ctlab_batch_destroy(ctlab_batch *b)
     if (!b) return set_status(CTLAB_OK, "");
     DeviceGuard dg(b->device);
     if (b->gexec) cudaGraphExecDestroy(b->gexec);
-    if (b->d_cases) cudaFree(b->d_cases);
     if (b->d_items) cudaFree(b->d_items);
     if (b->d_counter) cudaFree(b->d_counter);
-    if (b->h_cases) cudaFreeHost(b->h_cases);
+    for (cudaStream_t st : b->side) cudaStreamDestroy(st);
+    for (cudaEvent_t ev : b->join) cudaEventDestroy(ev);
+    if (b->fork) cudaEventDestroy(b->fork);
     delete b;
     return set_status(CTLAB_OK, "");
 }
@@ -305,9 +385,19 @@ static int batch_enqueue(ctlab_batch *b, const float *const *d_vols, const unsig
         int rc = plan_volume_sat(p, d_vols[i], d_masks ? d_masks[i] : nullptr, s);
         if (rc != CTLAB_OK) return rc;
     }
-    CTLAB_CUDA_TRY(cudaMemcpyAsync(b->d_cases, b->h_cases, sizeof(ProjBatchCase) * n, cudaMemcpyHostToDevice, s));
-    CTLAB_CUDA_TRY(cudaMemsetAsync(b->d_counter, 0, sizeof(int), s));
-    CTLAB_CUDA_TRY(launch_proj_t_batch(b->d_cases, b->d_items, b->nitems, b->d_counter, b->smem, b->grid, s));
+    const int nl = (int)b->launches.size();
+    CTLAB_CUDA_TRY(cudaMemsetAsync(b->d_counter, 0, sizeof(int) * nl, s));
+    // the launch with the most work first; the others wait for SMs it frees
+    if (nl > 1) CTLAB_CUDA_TRY(cudaEventRecord(b->fork, s));
+    for (int k = 0; k < nl; ++k) {
+        const BatchLaunch &l = b->launches[k];
+        cudaStream_t sk = k == 0 ? s : b->side[k - 1];
+        if (k > 0) CTLAB_CUDA_TRY(cudaStreamWaitEvent(sk, b->fork, 0));
+        CTLAB_CUDA_TRY(launch_proj_t_batch(l.nr, *l.params, b->d_items + l.first, l.count, b->d_counter + k, l.smem,
+                                           b->grid, sk));
+        if (k > 0) CTLAB_CUDA_TRY(cudaEventRecord(b->join[k - 1], sk));
+    }
+    for (int k = 1; k < nl; ++k) CTLAB_CUDA_TRY(cudaStreamWaitEvent(s, b->join[k - 1], 0));
     return CTLAB_OK;
 }
 
@@ -320,18 +410,20 @@ int ctlab_batch_proj(ctlab_batch *b, const float *const *d_vols, const unsigned 
         if (!d_vols[i] || !d_prjs[i]) return set_status(CTLAB_ERR_INVALID_ARG, "null volume or projection buffer");
     DeviceGuard dg(b->device);
     cudaStream_t s = (cudaStream_t)stream;
-    // the pinned case table is read by the copy at replay time: wait for the
-    // previous run before rewriting it
-    CTLAB_CUDA_TRY(cudaStreamSynchronize(s));
-    for (int i = 0; i < n; ++i) fill_case(b->plans[i], d_prjs[i], b->h_cases[i]);
+    // launch parameters: every case's arguments with its output buffer
+    for (BatchLaunch &l : b->launches)
+        for (size_t k = 0; k < l.cases.size(); ++k)
+            fill_case(b->plans[l.cases[k]], d_prjs[l.cases[k]], l.params->c[k]);
     if (!use_graph) {
         int rc = batch_enqueue(b, d_vols, d_masks, s);
         return rc == CTLAB_OK ? set_status(CTLAB_OK, "") : rc;
     }
+    // a graph replays the buffers it was captured with
     std::vector<const void *> ptrs;
     for (int i = 0; i < n; ++i) {
         ptrs.push_back(d_vols[i]);
         ptrs.push_back(d_masks ? d_masks[i] : nullptr);
+        ptrs.push_back(d_prjs[i]);
     }
     if (!b->gexec || ptrs != b->graph_ptrs) {
         if (b->gexec) {

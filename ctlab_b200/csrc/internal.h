@@ -234,8 +234,9 @@ struct ProjTStaging {
     bool ok = false;
 };
 // gcap limits the views per CTA (launches whose views group one by one use
-// a staging planned with gcap = 1); nstage > 0 fixes the stage depth.
-ProjTStaging proj_t_staging(const HostGeometry &g, int gcap = 16, int nstage = 0);
+// a staging planned with gcap = 1); nstage > 0 fixes the stage depth, zs > 0
+// the split of the detector rows over CTAs (1, 2 or 4).
+ProjTStaging proj_t_staging(const HostGeometry &g, int gcap = 16, int nstage = 0, int zs = 0);
 size_t proj_t_smem_bytes(const ProjTStaging &st);
 
 // One scan of a batched (persistent) projector launch: its arguments and TMA
@@ -244,9 +245,19 @@ struct __align__(64) ProjBatchCase {
     CUtensorMap tm_y, tm_x;
     ProjArgs a;
 };
-// Runs work items (case, detector tile, view group, row block) of the cases
-// on a persistent grid; *d_counter must be 0 (stream-ordered).
-cudaError_t launch_proj_t_batch(const ProjBatchCase *d_cases, const int4 *d_items, int nitems, int *d_counter,
+// The cases of one persistent launch, passed as a kernel parameter (so the
+// arguments and TMA maps sit in the constant bank like a single launch's).
+constexpr int kProjBatchMaxCases = 31000 / (int)sizeof(ProjBatchCase);
+struct ProjBatchParams {
+    ProjBatchCase c[kProjBatchMaxCases];
+};
+// Detector rows per consumer warp (nr) and warps per view (rb) of a launch
+// whose view groups hold G views under staging st.
+void proj_t_split(const ProjTStaging &st, int G, int &nr, int &rb);
+// Runs work items (case, detector tile, view group, row block) of up to
+// kProjBatchMaxCases cases whose launches have nr rows per consumer warp, on
+// a persistent grid; *d_counter must be 0 (stream-ordered).
+cudaError_t launch_proj_t_batch(int nr, const ProjBatchParams &cases, const int4 *d_items, int nitems, int *d_counter,
                                 size_t smem, int grid, cudaStream_t s);
 ProjGroups proj_t_make_groups(const HostGeometry &g, const std::vector<int> &list, const ProjTStaging &st);
 cudaError_t launch_proj_t(const ProjArgs &a, const ProjTStaging &st, const CUtensorMap &tmy, const CUtensorMap &tmx,

@@ -171,13 +171,8 @@ int plan_proj_list(ctlab_plan *p, const int *d_list, int n, const GroupTab &gt, 
         a.t_kb = st.KB;
         a.t_kr = st.KR;
         a.t_nstage = st.nstage;
-        // launches whose groups hold fewer views than planned keep the rows
-        // per CTA and split them over more warps (rows per warp >= 8)
-        int nr = st.NR, rb = st.RB;
-        while (gt.G * rb * 2 <= 16 && nr >= 16) {
-            nr /= 2;
-            rb *= 2;
-        }
+        int nr, rb;
+        proj_t_split(st, gt.G, nr, rb);
         a.t_rb = rb;
         a.t_nr = nr;
         a.t_zs = st.ZS;
@@ -399,7 +394,9 @@ int ctlab_plan_create(const ctlab_geometry *geom, int device, int sat_mode, ctla
     chk(dmalloc(&p->d_agg, state, bytes));
     chk(dmalloc(&p->d_pref, state, bytes));
     chk(dmalloc(&p->d_err, 1, bytes));
-    p->groups_cap = 2 * g.PN + 16;
+    // a view group table holds every run of views padded to whole groups:
+    // at most (views per group) entries per view
+    p->groups_cap = 16 * g.PN + 16;
     chk(dmalloc(&p->d_groups_all, (size_t)p->groups_cap, bytes));
     chk(dmalloc(&p->d_groups_scratch, (size_t)p->groups_cap, bytes));
     if (e != cudaSuccess) {

@@ -56,7 +56,7 @@ namespace {
 
 constexpr int kTU = 32;           // detector columns per CTA (one per lane)
 constexpr int kTMaxStage = 4;
-constexpr int kTMaxCWarps = 16;   // consumer warps
+constexpr int kTMaxCWarps = 15;   // consumer warps (16 warps with the producer: 128 registers a thread)
 constexpr int kTMaxG = 16;        // views per CTA
 constexpr int kTMaxThreads = (kTMaxCWarps + 1) * 32;
 constexpr size_t kTSmemLimit = 227 * 1024;
@@ -84,6 +84,98 @@ __device__ __forceinline__ float4 lds_f32x4(uint32_t addr)
     return v;
 }
 
+// z-interpolated column prefix at the row fraction fz: rows at pa and pa + RS4
+__device__ __forceinline__ float zinterp(uint32_t pa, uint32_t RS4, float fz)
+{
+    const float c0 = lds_f32(pa), c1 = lds_f32(pa + RS4);
+    return fmaf(fz, c1 - c0, c0);
+}
+
+// Staged slice address of the z-prefix row holding kz (clamped to the box),
+// and the fraction of kz past that row.  0 <= kz < 2^23, so adding 2^23
+// toward zero leaves floor(kz) in the mantissa bits; base folds in the box
+// origin and the 2^23 exponent bits.
+__device__ __forceinline__ uint32_t zrow_addr(float T, float e, float z0, float kzlo, float kzhi, uint32_t RS4,
+                                              uint32_t base, float &fz)
+{
+    float kz = fmaf(T, e, z0);
+    kz = fminf(fmaxf(kz, kzlo), kzhi);
+    const float rr = __fadd_rz(kz, 8388608.f);
+    fz = kz - (rr - 8388608.f);
+    return __float_as_uint(rr) * RS4 + base;
+}
+
+// Rows of one detector column on one slice when every strip of the warp
+// spans at most two voxel columns (a and b = a + dc, |dc| <= 1):
+// F(row boundary) = wa Z(a) + wb Z(b); acc[r] += (F(r + 1) - F(r)) scale.
+template <int NR>
+__device__ __forceinline__ void rows_narrow(float (&acc)[NR], const TEntry &te, int dc, uint32_t e_addr, uint32_t base,
+                                            uint32_t RS4, float z0, float kzlo, float kzhi)
+{
+    const uint32_t dc4 = 4u * (uint32_t)dc;
+    float prev = 0.f;
+#pragma unroll
+    for (int r4 = 0; r4 <= NR; r4 += 4) {
+        const float4 e4 = lds_f32x4(e_addr + 4u * r4);
+        const float ev[4] = {e4.x, e4.y, e4.z, e4.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = r4 + q;
+            if (r > NR) break;
+            float fz;
+            const uint32_t pa = zrow_addr(te.T, ev[q], z0, kzlo, kzhi, RS4, base, fz), pb = pa + dc4;
+            const float a0 = lds_f32(pa), a1 = lds_f32(pa + RS4);
+            const float b0 = lds_f32(pb), b1 = lds_f32(pb + RS4);
+            const float F = fmaf(te.wb, fmaf(fz, b1 - b0, b0), te.wa * fmaf(fz, a1 - a0, a0));
+            if (r > 0) acc[r - 1] = fmaf(F - prev, te.scale, acc[r - 1]);
+            prev = F;
+        }
+    }
+}
+
+// Weight of column a + i sgn(dc) in a strip from column a to column a + dc:
+// wa at a, wb at the far column, +-1 for the whole columns between, 0 past
+// the strip (those lanes read column a + dc again).
+__device__ __forceinline__ float strip_weight(const TEntry &te, int i, int dc, int adc)
+{
+    return i == 0 ? te.wa : (i < adc ? (dc > 0 ? 1.f : -1.f) : (i == adc ? te.wb : 0.f));
+}
+
+// Rows of one detector column when the warp's widest strip spans M + 1
+// voxel columns: one pass over the columns a .. a + M sgn(dc) per row.
+template <int NR, int M>
+__device__ __forceinline__ void rows_wide(float (&acc)[NR], const TEntry &te, int dc, uint32_t e_addr, uint32_t base,
+                                          uint32_t RS4, float z0, float kzlo, float kzhi)
+{
+    const int adc = dc < 0 ? -dc : dc;
+    const int step4 = dc < 0 ? -4 : 4;
+    float w[M + 1];
+    uint32_t off[M + 1];
+#pragma unroll
+    for (int i = 0; i <= M; ++i) {
+        w[i] = strip_weight(te, i, dc, adc);
+        off[i] = (uint32_t)(min(i, adc) * step4);
+    }
+    float prev = 0.f;
+#pragma unroll
+    for (int r4 = 0; r4 <= NR; r4 += 4) {
+        const float4 e4 = lds_f32x4(e_addr + 4u * r4);
+        const float ev[4] = {e4.x, e4.y, e4.z, e4.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int r = r4 + q;
+            if (r > NR) break;
+            float fz;
+            const uint32_t pa = zrow_addr(te.T, ev[q], z0, kzlo, kzhi, RS4, base, fz);
+            float F = w[0] * zinterp(pa, RS4, fz);
+#pragma unroll
+            for (int i = 1; i <= M; ++i) F = fmaf(w[i], zinterp(pa + off[i], RS4, fz), F);
+            if (r > 0) acc[r - 1] = fmaf(F - prev, te.scale, acc[r - 1]);
+            prev = F;
+        }
+    }
+}
+
 // Shared state of one projector tile besides the stage ring.
 struct ProjTShm {
     uint64_t full[kTMaxStage], empty[kTMaxStage];
@@ -99,9 +191,10 @@ struct ProjTShm {
 // One CTA's work: detector tile bx (32 columns), view group by, row block bz
 // of the launch described by a.  smem: the 128-byte aligned dynamic shared
 // memory (stages and z-boundary tables).
-template <int NR>
+template <int NR, bool kBatch>
 __device__ __forceinline__ void proj_t_tile(const ProjArgs &a, const CUtensorMap *tm_y_p, const CUtensorMap *tm_x_p,
-                                            int bx, int by, int bz, unsigned char *smem, ProjTShm &sh)
+                                            int bx, int by, int bz, unsigned char *smem, ProjTShm &sh,
+                                            const int4 *s_w)
 {
     const int G = a.G, RB = a.t_rb, NWC = G * RB;
     const int vbase = bz * RB * NR; // first detector row of this CTA (rows split over CTAs)
@@ -290,7 +383,7 @@ __device__ __forceinline__ void proj_t_tile(const ProjArgs &a, const CUtensorMap
                     atomicExch(a.err, CTLAB_ERR_TIMEOUT);
     } else if (warp < NWC && s_pos_list[warp / RB] >= 0) {
         // ------------------------------ consumers -----------------------------
-        const int g = warp / RB, v0l = (warp - g * RB) * NR, v0 = vbase + v0l;
+        const int g = warp / RB, v0l = (warp - g * RB) * NR;
         const float *zt = xdrv ? a.zt_x : a.zt_y;
         const int zrs = xdrv ? a.zt_rs_x : a.zt_rs_y;
         const float z0 = s_Z0[g];
@@ -336,62 +429,28 @@ __device__ __forceinline__ void proj_t_tile(const ProjArgs &a, const CUtensorMap
                 break;
             }
             const TSlice in = s_info[b];
-            const int2 cd = make_int2(in.fits ? ia - in.c_lo : ia, dc);
-            const bool wide = __any_sync(0xffffffffu, dc > 1 || dc < -1);
-            if (in.fits) {
+            // widest strip of the warp, in columns past column a (warp-uniform);
+            // strips of more than four columns (very coarse cells) read the
+            // column prefixes from global memory
+            const int adc = dc < 0 ? -dc : dc;
+            const int m = (int)__reduce_max_sync(0xffffffffu, (unsigned)adc);
+            const bool wide = m > 1;
+            const bool staged = in.fits && m <= 3;
+            const int2 cd = make_int2(staged ? ia - in.c_lo : ia, dc);
+            if (staged) {
                 // address of row k, column a = bits(k + 2^23) * RS4 + base (mod 2^32)
                 const uint32_t base = stage_addr + (uint32_t)b * 4u * (uint32_t)stage_floats + 4u * (uint32_t)cd.x -
                                       (uint32_t)in.k_lo * RS4 - 0x4B000000u * RS4;
-                const uint32_t dc4 = 4u * (uint32_t)dc;
                 const float kzlo = in.kz_lo, kzhi = in.kz_hi;
-                float prev = 0.f;
-#pragma unroll
-                for (int r4 = 0; r4 <= NR; r4 += 4) {
-                    const float4 e4 = lds_f32x4(e_addr + 4u * r4);
-                    const float ev[4] = {e4.x, e4.y, e4.z, e4.w};
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const int r = r4 + q;
-                        if (r > NR) break;
-                        float kz = fmaf(te.T, ev[q], z0);
-                        kz = fminf(fmaxf(kz, kzlo), kzhi);
-                        // 0 <= kz < 2^23: adding 2^23 toward zero leaves floor(kz) in the mantissa
-                        const float rr = __fadd_rz(kz, 8388608.f);
-                        const float fz = kz - (rr - 8388608.f);
-                        const uint32_t pa = __float_as_uint(rr) * RS4 + base, pb = pa + dc4;
-                        const float a0 = lds_f32(pa), a1 = lds_f32(pa + RS4);
-                        const float b0 = lds_f32(pb), b1 = lds_f32(pb + RS4);
-                        const float F = fmaf(te.wb, fmaf(fz, b1 - b0, b0), te.wa * fmaf(fz, a1 - a0, a0));
-                        if (r > 0) acc[r - 1] = fmaf(F - prev, te.scale, acc[r - 1]);
-                        prev = F;
-                    }
-                }
-                if (wide) {
-                    // cells wider than a voxel column: the whole columns strictly
-                    // between a and b, signed like b - a
-                    const int n = dc > 1 ? dc - 1 : (dc < -1 ? -dc - 1 : 0);
-                    const int step4 = dc > 0 ? 4 : -4;
-                    const float sgn_scale = dc > 0 ? te.scale : -te.scale;
-                    float prevx = 0.f;
-#pragma unroll
-                    for (int r = 0; r <= NR; ++r) {
-                        float kz = fmaf(te.T, lds_f32(e_addr + 4u * r), z0);
-                        kz = fminf(fmaxf(kz, kzlo), kzhi);
-                        const float rr = __fadd_rz(kz, 8388608.f);
-                        const float fz = kz - (rr - 8388608.f);
-                        const uint32_t pa = __float_as_uint(rr) * RS4 + base;
-                        float sum = 0.f;
-                        for (int i = 1; i <= n; ++i) {
-                            const uint32_t pc = pa + (uint32_t)(i * step4);
-                            const float c0 = lds_f32(pc), c1 = lds_f32(pc + RS4);
-                            sum += fmaf(fz, c1 - c0, c0);
-                        }
-                        if (r > 0) acc[r - 1] = fmaf(sum - prevx, sgn_scale, acc[r - 1]);
-                        prevx = sum;
-                    }
-                }
+                if (m <= 1)
+                    rows_narrow<NR>(acc, te, dc, e_addr, base, RS4, z0, kzlo, kzhi);
+                else if (m == 2)
+                    rows_wide<NR, 2>(acc, te, dc, e_addr, base, RS4, z0, kzlo, kzhi);
+                else
+                    rows_wide<NR, 3>(acc, te, dc, e_addr, base, RS4, z0, kzlo, kzhi);
             } else {
-                // block wider than a stage: the column prefixes from global memory
+                // block wider than a stage, or strips wider than four columns:
+                // the column prefixes from global memory
                 const float *S = zt + (long long)j * (ZN + 1) * zrs;
                 float prev = 0.f;
 #pragma unroll
@@ -422,32 +481,47 @@ __device__ __forceinline__ void proj_t_tile(const ProjArgs &a, const CUtensorMap
             if (lane == 0) mbar_arrive(&s_empty[b]);
         }
 
-        // epilogue: NR consecutive detector rows of column u per thread
+        // epilogue: NR consecutive detector rows of column u per thread.  A
+        // persistent (batch) CTA re-reads its arguments and work item here
+        // instead of holding them in registers across the slice loop.
+        const ProjArgs *ap = &a;
+        int ebx = bx, ebz = bz;
+        if (kBatch) {
+            asm volatile("" : "+l"(ap));
+            ebx = *reinterpret_cast<const volatile int *>(&s_w->y);
+            ebz = *reinterpret_cast<const volatile int *>(&s_w->w);
+        }
+        const ProjArgs &ae = *ap;
+        const int eu0 = ebx * kTU, enu = min(kTU, ae.DNU - eu0);
+        const int eDNV = ae.DNV, ev0 = ebz * ae.t_rb * NR + v0l;
+        const DetTable et = det_table_layout(ae.DNU, eDNV);
+        const double *edet = ae.det;
         const int li = s_pos_list[g];
-        if (lane < nu) {
-            const DevView &V = view_of(g);
-            const int u = u0 + lane;
-            const double lx = det[t.off_ux + u], ly = det[t.off_uy + u];
+        if (lane < enu) {
+            const int ps = li >= 0 ? li : s_pos_list[0];
+            const DevView &V = ae.views[ae.view_list[ps]];
+            const int u = eu0 + lane;
+            const double lx = edet[et.off_ux + u], ly = edet[et.off_uy + u];
             const double cx = lx * V.c - ly * V.s, cy = lx * V.s + ly * V.c;
             const double ex = cx - V.Sx, ey = cy - V.Sy;
             const double ea = V.xdrv ? ex : ey;
             const double e2 = ex * ex + ey * ey;
 #pragma unroll
             for (int r = 0; r < NR; ++r) {
-                const int v = v0 + r;
-                if (v < DNV) {
-                    const double ez = det[t.off_vz + v] + V.zP - V.Sz;
-                    const double L = dx * sqrt(e2 + ez * ez) / fabs(ea);
-                    const double de = (det[t.off_bz + v + 1] - det[t.off_bz + v]) / a.dz;
+                const int v = ev0 + r;
+                if (v < eDNV) {
+                    const double ez = edet[et.off_vz + v] + V.zP - V.Sz;
+                    const double L = ae.dx * sqrt(e2 + ez * ez) / fabs(ea);
+                    const double de = (edet[et.off_bz + v + 1] - edet[et.off_bz + v]) / ae.dz;
                     const float val = (float)((double)acc[r] * (L / de));
-                    const long long idx = ((long long)li * a.DNU + u) * DNV + v;
-                    if (a.epilogue == PROJ_SART_RESIDUAL) {
-                        const float mv = a.meas[idx], rsum = a.row_sum[idx];
+                    const long long idx = ((long long)li * ae.DNU + u) * eDNV + v;
+                    if (ae.epilogue == PROJ_SART_RESIDUAL) {
+                        const float mv = ae.meas[idx], rsum = ae.row_sum[idx];
                         const float res = mv - val;
                         r2 += (double)res * (double)res;
-                        a.out[idx] = (rsum > 1.0e-7f) ? res / rsum : 0.f;
+                        ae.out[idx] = (rsum > 1.0e-7f) ? res / rsum : 0.f;
                     } else {
-                        a.out[idx] = val;
+                        ae.out[idx] = val;
                     }
                 }
             }
@@ -478,41 +552,33 @@ __global__ void __launch_bounds__(kTMaxThreads, 1)
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ ProjTShm sh;
     // TMA destinations need 128-byte alignment (the launch adds 128 bytes)
-    proj_t_tile<NR>(a, &tm_y, &tm_x, blockIdx.x, blockIdx.y, blockIdx.z, align128(smem_raw), sh);
+    proj_t_tile<NR, false>(a, &tm_y, &tm_x, blockIdx.x, blockIdx.y, blockIdx.z, align128(smem_raw), sh, nullptr);
 }
 
 // Persistent projector over many scans: CTAs take (case, tile, group, row
 // block) work items from a queue (items sorted longest first) and run them
-// with each case's arguments and TMA maps from global memory.
+// with each case's arguments and TMA maps from the kernel parameters.  Every
+// case of one launch has NR detector rows per consumer warp.
+template <int NR>
 __global__ void __launch_bounds__(kTMaxThreads, 1)
-    dd3_proj_t_batch_kernel(const ProjBatchCase *__restrict__ cases, const int4 *__restrict__ items, int nitems,
+    dd3_proj_t_batch_kernel(const __grid_constant__ ProjBatchParams cases, const int4 *__restrict__ items, int nitems,
                             int *counter)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ ProjTShm sh;
-    __shared__ ProjArgs s_a;
-    __shared__ int s_item;
+    __shared__ int4 s_w;
     unsigned char *smem = align128(smem_raw);
     const int tid = threadIdx.x;
     for (;;) {
-        if (tid == 0) s_item = atomicAdd(counter, 1);
-        __syncthreads();
-        const int it = s_item;
-        if (it >= nitems) break;
-        const int4 w = items[it];
-        const ProjBatchCase &c = cases[w.x];
-        {
-            const int *src = reinterpret_cast<const int *>(&c.a);
-            int *dst = reinterpret_cast<int *>(&s_a);
-            for (int i = tid; i < (int)(sizeof(ProjArgs) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+        if (tid == 0) {
+            const int it = atomicAdd(counter, 1);
+            s_w = it < nitems ? items[it] : make_int4(-1, 0, 0, 0);
         }
         __syncthreads();
-        switch (s_a.t_nr) {
-        case 4: proj_t_tile<4>(s_a, &c.tm_y, &c.tm_x, w.y, w.z, w.w, smem, sh); break;
-        case 8: proj_t_tile<8>(s_a, &c.tm_y, &c.tm_x, w.y, w.z, w.w, smem, sh); break;
-        case 16: proj_t_tile<16>(s_a, &c.tm_y, &c.tm_x, w.y, w.z, w.w, smem, sh); break;
-        default: proj_t_tile<32>(s_a, &c.tm_y, &c.tm_x, w.y, w.z, w.w, smem, sh); break;
-        }
+        const int4 w = s_w;
+        if (w.x < 0) break;
+        const ProjBatchCase &c = cases.c[w.x];
+        proj_t_tile<NR, true>(c.a, &c.tm_y, &c.tm_x, w.y, w.z, w.w, smem, sh, &s_w);
         // every warp is done with this item's barriers and buffers
         __syncthreads();
         if (tid < kTMaxStage) {
@@ -659,32 +725,52 @@ int env_int(const char *name, int dflt)
 
 size_t proj_t_smem_bytes(const ProjTStaging &st) { return smem_bytes(st); }
 
-cudaError_t launch_proj_t_batch(const ProjBatchCase *d_cases, const int4 *d_items, int nitems, int *d_counter,
-                                size_t smem, int grid, cudaStream_t s)
+template <int NR>
+cudaError_t launch_batch_nr(const ProjBatchParams &cases, const int4 *d_items, int nitems, int *d_counter, size_t smem,
+                            int grid, cudaStream_t s)
 {
-    if (nitems <= 0) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(dd3_proj_t_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    auto kern = dd3_proj_t_batch_kernel<NR>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    dd3_proj_t_batch_kernel<<<grid, kTMaxThreads, smem, s>>>(d_cases, d_items, nitems, d_counter);
+    kern<<<grid, kTMaxThreads, smem, s>>>(cases, d_items, nitems, d_counter);
     return cudaGetLastError();
 }
 
-ProjTStaging proj_t_staging(const HostGeometry &g, int gcap, int nstage_fix)
+cudaError_t launch_proj_t_batch(int nr, const ProjBatchParams &cases, const int4 *d_items, int nitems, int *d_counter,
+                                size_t smem, int grid, cudaStream_t s)
+{
+    if (nitems <= 0) return cudaSuccess;
+    switch (nr) {
+    case 4: return launch_batch_nr<4>(cases, d_items, nitems, d_counter, smem, grid, s);
+    case 8: return launch_batch_nr<8>(cases, d_items, nitems, d_counter, smem, grid, s);
+    case 12: return launch_batch_nr<12>(cases, d_items, nitems, d_counter, smem, grid, s);
+    case 16: return launch_batch_nr<16>(cases, d_items, nitems, d_counter, smem, grid, s);
+    case 20: return launch_batch_nr<20>(cases, d_items, nitems, d_counter, smem, grid, s);
+    case 24: return launch_batch_nr<24>(cases, d_items, nitems, d_counter, smem, grid, s);
+    case 28: return launch_batch_nr<28>(cases, d_items, nitems, d_counter, smem, grid, s);
+    case 32: return launch_batch_nr<32>(cases, d_items, nitems, d_counter, smem, grid, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+ProjTStaging proj_t_staging(const HostGeometry &g, int gcap, int nstage_fix, int zs_fix)
 {
     ProjTStaging st;
     st.ok = false;
-    // CTLAB_PROJT_GMAX caps the views per CTA (1..16), CTLAB_PROJT_ZS fixes
+    // CTLAB_PROJT_GMAX caps the views per CTA (1..15), CTLAB_PROJT_ZS fixes
     // the row split (1, 2, 4), CTLAB_PROJT_NSTAGE the stage depth (2..4),
     // CTLAB_PROJT_CBMAX caps the staged columns
-    const int gmax = std::max(1, std::min(std::min(env_int("CTLAB_PROJT_GMAX", 8), kTMaxG), gcap));
-    const int want_zs = env_int("CTLAB_PROJT_ZS", 0);
+    const int gmax = std::max(1, std::min(std::min(env_int("CTLAB_PROJT_GMAX", kTMaxCWarps), kTMaxG), gcap));
+    const int want_zs = zs_fix > 0 ? zs_fix : env_int("CTLAB_PROJT_ZS", 0);
     const int want_stage = nstage_fix > 0 ? nstage_fix : env_int("CTLAB_PROJT_NSTAGE", 0);
     const int cbmax = std::min(env_int("CTLAB_PROJT_CBMAX", 256), 256);
     std::vector<int> all(g.PN);
     for (int i = 0; i < g.PN; ++i) all[i] = i;
-    for (int G = kTMaxG; G >= 1; G /= 2) {
-        if (G > gmax) continue;
+    // candidates (views per CTA, row split): prefer >= 12 consumer warps, then
+    // more views per CTA, then fewer row splits
+    ProjTStaging best;
+    int best_key = -1;
+    for (int G = gmax; G >= 1; --G) {
         int CB = (t_need(g, as_views(t_groups(g, all, G), all)) + 3) & ~3;
         // a row stride of 16 (mod 32) floats keeps lanes that read neighbouring
         // rows off each other's banks; take it when it costs little
@@ -698,12 +784,15 @@ ProjTStaging proj_t_staging(const HostGeometry &g, int gcap, int nstage_fix)
             if (want_zs && ZS != want_zs) continue;
             if (!want_zs && ZS > 1 && g.DNV < 16 * ZS) continue;
             const int rows = (g.DNV + ZS - 1) / ZS; // detector rows per CTA
-            // rows per consumer warp: 8..32 (4 for tiny detectors), the row
-            // blocks of G views filling at most 16 warps
-            int NR = rows >= 64 ? 8 : 4;
-            while ((rows + NR - 1) / NR * G > kTMaxCWarps && NR < 32) NR *= 2;
-            const int RB = (rows + NR - 1) / NR;
+            // warps per view: as many as the consumer warps allow while each
+            // keeps >= 8 rows, at least enough for <= 32 rows per warp; rows
+            // per warp: the rows split evenly, rounded up to 4
+            const int rb_min = (rows + 31) / 32;
+            const int RB = std::max(rb_min, std::min(kTMaxCWarps / G, (rows + 7) / 8));
             if (RB * G > kTMaxCWarps) continue;
+            const int NR = std::min(32, ((rows + RB - 1) / RB + 3) & ~3);
+            const int key = (RB * G >= 12 ? 1000 : 0) + G * 10 + (4 - ZS);
+            if (key <= best_key) continue;
             const int zs = (g.DNV + RB * NR - 1) / (RB * NR); // CTAs over the rows (no empty one)
             // z rows a CTA stages per slice: the clamped kz range of its
             // detector rows over the group's views and the tile's columns
@@ -728,16 +817,24 @@ ProjTStaging proj_t_staging(const HostGeometry &g, int gcap, int nstage_fix)
                 c.smem = smem_bytes(c);
                 if (c.smem + kTStatic > kTSmemLimit) continue;
                 c.ok = true;
-                return c;
+                best = c;
+                best_key = key;
+                break;
             }
         }
+        // a candidate with enough warps beats every smaller group size
+        if (best_key >= 1000) break;
     }
+    if (best.ok) return best;
     // nothing stages: every slice reads global memory
     st.G = 1;
     st.ZS = 1;
-    st.NR = 4;
-    while ((g.DNV + st.NR - 1) / st.NR > kTMaxCWarps) st.NR *= 2;
-    st.RB = (g.DNV + st.NR - 1) / st.NR;
+    const int splits = (g.DNV + kTMaxCWarps * 32 - 1) / (kTMaxCWarps * 32);
+    const int per = (g.DNV + splits - 1) / splits; // rows per CTA
+    st.RB = std::min(kTMaxCWarps, std::max((per + 31) / 32, (per + 7) / 8));
+    st.NR = std::min(32, ((per + st.RB - 1) / st.RB + 3) & ~3);
+    st.RB = (per + st.NR - 1) / st.NR;
+    st.ZS = (g.DNV + st.RB * st.NR - 1) / (st.RB * st.NR);
     st.CB = 0;
     st.KB = 0;
     st.KR = 0;
@@ -764,6 +861,18 @@ ProjGroups proj_t_make_groups(const HostGeometry &g, const std::vector<int> &lis
     return out;
 }
 
+void proj_t_split(const ProjTStaging &st, int G, int &nr, int &rb)
+{
+    // launches whose groups hold fewer views than planned keep the rows per
+    // CTA and split them over more warps (rows per warp >= 8, a multiple of 4)
+    nr = st.NR;
+    rb = st.RB;
+    while (G * rb * 2 <= kTMaxCWarps && nr >= 16 && nr % 8 == 0) {
+        nr /= 2;
+        rb *= 2;
+    }
+}
+
 cudaError_t launch_proj_t(const ProjArgs &a, const ProjTStaging &st, const CUtensorMap &tmy, const CUtensorMap &tmx,
                           cudaStream_t s, int *launches)
 {
@@ -775,7 +884,11 @@ cudaError_t launch_proj_t(const ProjArgs &a, const ProjTStaging &st, const CUten
     switch (a.t_nr) {
     case 4: return launch_t_nr<4>(a, tmy, tmx, sm, s);
     case 8: return launch_t_nr<8>(a, tmy, tmx, sm, s);
+    case 12: return launch_t_nr<12>(a, tmy, tmx, sm, s);
     case 16: return launch_t_nr<16>(a, tmy, tmx, sm, s);
+    case 20: return launch_t_nr<20>(a, tmy, tmx, sm, s);
+    case 24: return launch_t_nr<24>(a, tmy, tmx, sm, s);
+    case 28: return launch_t_nr<28>(a, tmy, tmx, sm, s);
     case 32: return launch_t_nr<32>(a, tmy, tmx, sm, s);
     default: return cudaErrorInvalidValue;
     }

@@ -102,7 +102,7 @@ int ctlab_os_sart(ctlab_plan *plan, float *d_x, const float *d_meas, const unsig
     const long long nd = (long long)g.DNU * g.DNV;
     const long long nv = (long long)g.XN * g.YN * g.ZN;
     DevBuf d_order, d_bsub, d_rows, d_cols, d_r, d_ones, d_acc, d_est, d_groups;
-    const int gcap = 2 * g.PN + 16;
+    const int gcap = plan->groups_cap;
     int rc = alloc(d_order, sizeof(int) * g.PN);
     if (rc == CTLAB_OK) rc = alloc(d_groups, sizeof(int) * (size_t)gcap * (os_num + 1));
     if (rc == CTLAB_OK) rc = alloc(d_bsub, sizeof(float) * nd * g.PN);

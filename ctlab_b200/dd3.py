@@ -154,6 +154,14 @@ class Plan:
                                            None if cache_path is None else cache_path.encode(), C.byref(ms)))
         return ms.value
 
+    def proj_tiles(self) -> dict:
+        """The z-prefix projector's staging (views per CTA, rows per warp, ...)."""
+        t = (C.c_int * 8)()
+        check(self.lib.ctlab_plan_proj_tiles(self.handle, t))
+        keys = ("views_per_cta", "rows_per_warp", "warps_per_view", "z_splits", "box_cols", "box_rows",
+                "stages", "ctas")
+        return dict(zip(keys, list(t)))
+
     def proj(self, vol, out, mask=None, stream=None):
         check(self.lib.ctlab_proj(self.handle, self._p(vol), self._p(mask), self._p(out), self._stream(stream)))
         return out

@@ -255,6 +255,12 @@ int ctlab_sart_back_weight(float *d_vol, float *d_recon, const float *d_col_sum,
 int ctlab_plan_autotune(ctlab_plan *plan, const float *d_vol, float *d_prj, const char *cache_path,
                         float *best_ms);
 
+/* The projector staging of a z-prefix plan: tiles[0..7] = views per CTA,
+ * detector rows per consumer warp, consumer warps per view, z splits, staged
+ * columns per box, staged z-prefix rows per box, stage depth, and the CTAs of
+ * a projection of all views. */
+int ctlab_plan_proj_tiles(const ctlab_plan *plan, int *tiles);
+
 /* A batch projects the scans of n z-prefix plans (one device) together. */
 typedef struct ctlab_batch ctlab_batch;
 int ctlab_batch_create(ctlab_plan *const *plans, int n, ctlab_batch **out);
@@ -266,8 +272,7 @@ long long ctlab_batch_voxel_views(const ctlab_batch *batch);
  * launch over the work items of all cases (sorted longest first).  With
  * use_graph the sequence is captured into a CUDA graph on the first call
  * (stream must not be the legacy default stream) and replayed while the
- * volume and mask pointers stay the same.  Waits for the stream's previous
- * work before it rewrites its case table. */
+ * volume, mask and projection pointers stay the same. */
 int ctlab_batch_proj(ctlab_batch *batch, const float *const *d_vols, const unsigned char *const *d_masks,
                      float *const *d_prjs, int use_graph, void *stream);
 
