@@ -46,11 +46,12 @@ def parse():
     ap.add_argument("--cpu-views", type=int, default=4, help="views in the bounded CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="dd3", choices=["dd3", "recon", "learned", "batch"],
+    ap.add_argument("--workload", default="dd3", choices=["dd3", "recon", "learned", "batch", "helical"],
                     help="dd3: the projector/backprojector throughput line (default); recon: OS-SART 24x30 and "
                          "FISTA-TV 50 at 256x256x128 / 720 views with residual and RMSE per iteration; learned: "
                          "train the warm-start CNN on OS-SART 2- vs 30-iteration pairs, then time-to-residual "
-                         "learned vs plain")
+                         "learned vs plain; batch: 48 uneven scans, one persistent launch vs per-scan launches; "
+                         "helical: projection and backprojection of a 512x512x1024 helical scan")
     ap.add_argument("--train-volumes", type=int, default=16, help="learned workload: training phantoms")
     ap.add_argument("--train-steps", type=int, default=1500, help="learned workload: Adam steps")
     ap.add_argument("--recon-iters", type=int, default=0,
@@ -618,10 +619,59 @@ def run_batch(args):
         p.close()
 
 
+def run_helical(args):
+    """Projection and backprojection of a long helical scan (512x512x1024 at 1 x 1 x 0.5
+    mm, 14 turns of 984 views, pitch 1, the 888x64 detector): each view's cone meets a
+    short z slab of the volume, so backprojector CTAs whose z range the cone misses skip
+    the view.  Device times with CUDA events; inputs larger than L2."""
+    import torch
+
+    import ctlab_b200 as cb
+    from ctlab_b200 import geometry as G
+
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    g = G.helical()
+    hx, hy, hz = G.half_extents(g)
+    vol = torch.zeros(g.vol_shape, dtype=torch.float32, device="cuda")
+    cb.ellipsoid_phantom(vol, g, cb.random_ellipsoids(21, hx, hy, hz))
+    prj = torch.zeros(g.prj_shape, dtype=torch.float32, device="cuda")
+    back = torch.zeros(g.vol_shape, dtype=torch.float32, device="cuda")
+    plan = cb.Plan(g, device=local)
+    plan.set_timing(True)
+    steps, warm = max(1, min(args.steps, 2)), max(1, min(args.warmup, 1))
+    times = []
+    with ClockSampler(local) as clk:
+        for it in range(warm + steps):
+            plan.proj(vol, prj)
+            torch.cuda.synchronize()
+            ps, pg = plan.last_times()
+            plan.back(prj, back)
+            torch.cuda.synchronize()
+            bs, bg = plan.last_times()
+            if it >= warm:
+                times.append((ps, pg, bs, bg))
+    t = np.array(times).mean(axis=0)
+    vv = g.voxel_views
+    line = {"metric": "helical projection / backprojection time", "workload": "helical_512x512x1024_13776v_888x64",
+            "n_gpus": 1, "data": "synthetic (seeded random-ellipsoid phantom)", "views": g.PN,
+            "volume": [g.XN, g.YN, g.ZN], "voxel_mm": [g.dx, g.dx, g.dz], "pitch": 1.0,
+            "proj_ms": float(t[0] + t[1]), "back_ms": float(t[2] + t[3]),
+            "kernels_ms": {"proj_sat": float(t[0]), "proj": float(t[1]), "back_sat": float(t[2]), "back": float(t[3])},
+            "gvoxel_views_per_s": {"proj": vv / ((t[0] + t[1]) * 1e-3) / 1e9, "back": vv / ((t[2] + t[3]) * 1e-3) / 1e9},
+            "steps": steps, "warmup": warm, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    plan.close()
+
+
 def main():
     args = parse()
     if args.workload == "batch":
         run_batch(args)
+    elif args.workload == "helical":
+        run_helical(args)
     elif args.workload == "recon":
         run_recon(args)
     elif args.workload == "learned":

@@ -115,7 +115,7 @@ __device__ __forceinline__ double u_of(const DevView &V, double px, double py)
     return cross2(V.Sx - V.B0x, V.Sy - V.B0y, dpx, dpy) / cross2(V.Ex, V.Ey, dpx, dpy);
 }
 
-template <int KSEG, int VPT>
+template <int KSEG, int VPT, bool ZSKIP>
 __global__ void __launch_bounds__(kThreads, 1) dd3_back_t_kernel(BackArgs a, int es2, int rmax)
 {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -127,6 +127,7 @@ __global__ void __launch_bounds__(kThreads, 1) dd3_back_t_kernel(BackArgs a, int
     __shared__ double s_u[kGeo][kB][kB + 1];
     __shared__ float s_V0[kGeo][kCols], s_V1[kGeo][kCols];
     __shared__ int s_xdrv[kGeo];
+    __shared__ int s_cov[kGeo][2]; // the view's cone meets this CTA's z range (per column half)
 
     const int tid = threadIdx.x;
     const int bx0 = blockIdx.x * kB, by0 = blockIdx.y * kB;
@@ -144,6 +145,8 @@ __global__ void __launch_bounds__(kThreads, 1) dd3_back_t_kernel(BackArgs a, int
     const long long pstride = (long long)DNU * vp;
     const float DNVf = (float)DNV;
     const double inv_n = 1.0 / (a.dzb * DNV), dz_n = a.dz * inv_n; // detector rows, normalised by DNV
+    // z boundaries this CTA's phase B samples (its segments' k0 .. k0 + KSEG)
+    const float kz_lo = (float)(blockIdx.z * (kZS * KSEG)), kz_hi = kz_lo + (float)(kZS * KSEG);
 
     if (tid == 0) {
         mbar_init(&s_bar[0], 1);
@@ -178,8 +181,19 @@ __global__ void __launch_bounds__(kThreads, 1) dd3_back_t_kernel(BackArgs a, int
                               cross2(pcx - V.Sx, pcy - V.Sy, V.Ex, V.Ey);
             const double zb0 = zb0_local + V.zP;
             // z boundary k' -> detector row coordinate v = V0 + V1 k', stored / DNV
-            s_V1[sl][c] = (float)(tc * dz_n);
-            s_V0[sl][c] = (float)((V.Sz + tc * (a.z_lo - V.Sz) - zb0) * inv_n);
+            const float V1 = (float)(tc * dz_n), V0 = (float)((V.Sz + tc * (a.z_lo - V.Sz) - zb0) * inv_n);
+            s_V1[sl][c] = V1;
+            s_V0[sl][c] = V0;
+            if (ZSKIP) {
+                // does this column's z range [kz_lo, kz_hi] reach a detector
+                // row?  Outside, every boundary saturates to the same end of
+                // the column and the view adds exactly 0 (a helical scan's
+                // views far along z)
+                const float va = fmaf(V1, kz_lo, V0), vb = fmaf(V1, kz_hi, V0);
+                const bool meets = fmaxf(va, vb) > -1e-3f && fminf(va, vb) < 1.f + 1e-3f;
+                const unsigned any = __ballot_sync(0xffffffffu, meets);
+                if ((tid & 31) == 0) s_cov[sl][(tid - 128) >> 5] = any != 0u;
+            }
         }
     };
     // staging of list entry l into buffer l & 1 (thread 0): the rows of P the
@@ -193,9 +207,10 @@ __global__ void __launch_bounds__(kThreads, 1) dd3_back_t_kernel(BackArgs a, int
         // one row of margin each side: interior boundaries may round past
         // the corners' range by an ulp
         const int lo = max((int)umin - 1, 0), rows = min((int)umax + 2, DNU - 1) - lo + 1;
-        const bool fits = rows <= rmax;
+        const bool meets = !ZSKIP || s_cov[sl][0] || s_cov[sl][1];
+        const bool fits = meets && rows <= rmax;
         s_ulo[b] = lo;
-        s_rows[b] = fits ? rows : 0;
+        s_rows[b] = meets ? (fits ? rows : 0) : -1; // -1: the view misses the brick
         mbar_arrive_expect_tx(&s_bar[b], fits ? (uint32_t)(4 * rows * vp) : 0u);
         if (fits)
             bulk_copy_g2s(pbuf + (size_t)b * rmax * vp, Pall + l * pstride + (long long)lo * vp,
@@ -229,7 +244,7 @@ __global__ void __launch_bounds__(kThreads, 1) dd3_back_t_kernel(BackArgs a, int
         float2 *E = E2 + (size_t)b * kCols * es2; // double buffered: B(li) overlaps A(li+1)
 
         // ---- A: (E_c(i), E_c(i+1) - E_c(i)) for i in [0, DNV], E_c(DNV+1) = E_c(DNV) ----
-        if (!timed_out) {
+        if (!timed_out && (!ZSKIP || rows >= 0)) {
             const double ua = xdrv ? s_u[ls][acx][acy] : s_u[ls][acy][acx];
             const double ub = xdrv ? s_u[ls][acx][acy + 1] : s_u[ls][acy][acx + 1];
             const double uca = fmin(fmax(ua, 0.0), (double)DNU), ucb = fmin(fmax(ub, 0.0), (double)DNU);
@@ -312,7 +327,7 @@ __global__ void __launch_bounds__(kThreads, 1) dd3_back_t_kernel(BackArgs a, int
         geometry(li + 3);
 
         // ---- phase B: voxels ----
-        if (in_vol && !timed_out) {
+        if (in_vol && !timed_out && (!ZSKIP || rows >= 0)) {
             const float V0 = s_V0[ls][col], V1 = s_V1[ls][col];
             // address of (E, dE)_c[i] = bits(i + 2^23) * 8 + base (mod 2^32)
             const uint32_t base = E2_addr + 8u * (uint32_t)(b * kCols * es2 + col * es2) - 8u * 0x4B000000u;
@@ -396,12 +411,12 @@ size_t dyn_smem(int rmax, int vp, int es2)
     return 4 * 2 * (size_t)rmax * vp + sizeof(float2) * 2 * (size_t)kCols * es2;
 }
 
-template <int KSEG, int VPT>
+template <int KSEG, int VPT, bool ZSKIP>
 cudaError_t launch_k(const BackArgs &a, cudaStream_t s)
 {
     const int es2 = e_pitch(a.DNV); // (E, dE) pairs per column, odd pitch
     const size_t sm = dyn_smem(a.rmax, a.vp, es2);
-    auto kern = dd3_back_t_kernel<KSEG, VPT>;
+    auto kern = dd3_back_t_kernel<KSEG, VPT, ZSKIP>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     dim3 grid((a.XN + kB - 1) / kB, (a.YN + kB - 1) / kB, (a.ZN + kZS * KSEG - 1) / (kZS * KSEG));
@@ -409,13 +424,17 @@ cudaError_t launch_k(const BackArgs &a, cudaStream_t s)
     return cudaGetLastError();
 }
 
+// Segment length by ZN; volumes of several z blocks (and helical scans with
+// 256-voxel blocks) test each view against each CTA's z range and skip the
+// views whose cone misses it.
 template <int VPT>
 cudaError_t launch_z(const BackArgs &a, cudaStream_t s)
 {
-    if (a.ZN <= kZS * 4) return launch_k<4, VPT>(a, s);
-    if (a.ZN <= kZS * 8) return launch_k<8, VPT>(a, s);
-    if (a.ZN <= kZS * 16) return launch_k<16, VPT>(a, s);
-    return launch_k<32, VPT>(a, s);
+    if (a.ZN <= kZS * 4) return launch_k<4, VPT, false>(a, s);
+    if (a.ZN <= kZS * 8) return launch_k<8, VPT, false>(a, s);
+    if (a.ZN <= kZS * 16) return launch_k<16, VPT, false>(a, s);
+    if (a.zskip || a.ZN > kZS * 32) return launch_k<32, VPT, true>(a, s);
+    return launch_k<32, VPT, false>(a, s);
 }
 
 } // namespace

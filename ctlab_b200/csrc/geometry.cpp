@@ -115,6 +115,8 @@ int build_geometry(const ctlab_geometry &g, HostGeometry &o)
     }
 
     o.views.resize(g.PN);
+    o.angle.resize(g.PN);
+    for (int p = 0; p < g.PN; ++p) o.angle[p] = (double)g.hangs[p];
     for (int p = 0; p < g.PN; ++p) {
         DevView &v = o.views[p];
         std::memset(&v, 0, sizeof v);
@@ -180,9 +182,9 @@ std::vector<std::vector<int>> view_runs(const HostGeometry &g, const std::vector
         for (int pos = 0; pos < (int)list.size(); ++pos) {
             const DevView &V = g.views[list[pos]];
             if (V.xdrv != axis) continue;
-            double th = std::atan2(V.s, V.c);
-            if (th < 0) th += kTwoPi;
-            ang.push_back({th, pos});
+            // the angle as given: views of different helical turns (different
+            // source z) at the same angle mod 2 pi are not neighbours
+            ang.push_back({g.angle[list[pos]], pos});
         }
         if (ang.empty()) continue;
         std::stable_sort(ang.begin(), ang.end(),

@@ -64,6 +64,7 @@ struct HostGeometry {
     std::vector<double> bx, by, bz; // local detector boundaries (DNU+1, DNU+1, DNV+1)
     std::vector<double> ux, uy, vz; // local detector centres (DNU, DNU, DNV)
     std::vector<DevView> views;
+    std::vector<double> angle; // view angles as given (unwrapped: helical turns stay apart)
     bool flat_uniform = false; // flat detector with uniform u and v pitch
     double dzb = 0;            // v pitch (flat_uniform)
 };
@@ -287,6 +288,7 @@ struct BackArgs {
     int rmax;             // staging-buffer SAT rows (back_staging_rows)
     int *err;             // device error word (bounded waits)
     const float *pv;      // projection v-prefixes [n][DNU][vp] (sat mode ZPREFIX)
+    int zskip;            // a helical scan: views may miss a CTA's z range (tested, then skipped)
 };
 cudaError_t launch_back(const BackArgs &a, cudaStream_t s, int *launches);
 // Backprojector on projection v-prefixes (sat mode ZPREFIX).

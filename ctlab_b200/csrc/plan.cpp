@@ -248,6 +248,8 @@ int plan_back_list(ctlab_plan *p, const int *d_list, int n, const unsigned char 
     a.rmax = p->back_rmax;
     a.err = p->d_err;
     a.pv = p->d_pv;
+    for (const DevView &V : g.views)
+        if (V.zP != g.views[0].zP) a.zskip = 1; // a helical scan
     if (n == 0 && epilogue == BACK_PLAIN) {
         CTLAB_CUDA_TRY(cudaMemsetAsync(d_vol, 0, sizeof(float) * (size_t)g.XN * g.YN * g.ZN, s));
         return CTLAB_OK;
@@ -318,7 +320,9 @@ int ctlab_plan_create(const ctlab_geometry *geom, int device, int sat_mode, ctla
         return rc;
     }
     const HostGeometry &g = p->g;
-    if (!proj_supported(g.ZN, g.DNV)) {
+    // the FP64 / float-pair projector stages whole SAT columns; the z-prefix
+    // projector stages z ranges and splits detector rows over CTAs
+    if (sat_mode != CTLAB_SAT_ZPREFIX && !proj_supported(g.ZN, g.DNV)) {
         delete p;
         return set_status(CTLAB_ERR_UNSUPPORTED, "ZN or DNV beyond the projector's shared-memory tiles");
     }

@@ -119,6 +119,22 @@ def config3() -> DD3Geometry:
                             XN=256, YN=256, ZN=128, dx=0.5, dz=0.5)
 
 
+def helical(XN: int = 512, YN: int = 512, ZN: int = 1024, dz: float = 0.5, views_per_turn: int = 984,
+            pitch: float = 1.0) -> DD3Geometry:
+    """Helical scan of a long volume (1 mm in-plane voxels, dz along z) with the 888x64
+    detector of config 2: the source advances pitch x the detector's z coverage at the
+    isocentre per turn, over the volume's z extent plus one coverage."""
+    DNU, DNV, col, row = 888, 64, 1.0239, 1.0960
+    coverage = DNV * row * SOD / SDD
+    span = ZN * dz + coverage
+    turns = math.ceil(span / (pitch * coverage))
+    PN = turns * views_per_turn
+    angles = 2.0 * math.pi * np.arange(PN) / views_per_turn
+    zpos = np.linspace(-0.5 * span, 0.5 * span, PN)
+    return DD3Geometry.flat(sid=SOD, sdd=SDD, DNU=DNU, DNV=DNV, col_size=col, row_size=row, PN=PN,
+                            XN=XN, YN=YN, ZN=ZN, dx=1.0, dz=dz, angles=angles, zpos=zpos)
+
+
 def config4(seed: int = 7, n: int = 48) -> list[DD3Geometry]:
     """The uneven batch: n scans with volumes from {128^3, 192x192x96, 256x256x64,
     384x384x32} (1 mm voxels), 180-720 views, detectors 256-768 cells wide and 32-64

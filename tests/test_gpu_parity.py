@@ -49,6 +49,9 @@ CASES = {
     "odd_offsets": dict(XN=23, YN=19, ZN=13, DNU=37, DNV=11, col_offset=0.37, row_offset=-0.21,
                         center=(1.3, -0.7, 0.4), start=0.05),
     "helical_shift": dict(PN=20, zpos=np.linspace(-1.5, 1.5, 20)),
+    # a long helical volume: each view's cone meets only part of the z range,
+    # so backprojector CTAs skip the views that miss their z slab
+    "helical_long": dict(PN=40, ZN=600, dz=0.05, zpos=np.linspace(-14.0, 14.0, 40)),
     "wide_z": dict(XN=9, YN=8, ZN=300, DNU=20, DNV=40, dz=0.05, row_size=0.1),
     "single_row": dict(DNV=1, row_size=0.5),
     "coarse_det": dict(DNU=9, DNV=5, col_size=4.0, row_size=3.0),
@@ -347,3 +350,29 @@ def test_bounded_wait_times_out_and_context_survives(torch_cuda):
         plan.proj(dev(torch, phantom(g)), out)
         torch.cuda.synchronize()
         assert float(out.abs().sum()) > 0
+
+
+@pytest.mark.parametrize("zpos", [None, "helical"])
+def test_zprefix_tall_volume_matches_oracle(torch_cuda, zpos):
+    """A volume longer than the cone (ZN = 1200, several backprojector z blocks, beyond
+    the FP64 projector's shared-memory columns): the z-prefix projector stages z ranges,
+    and backprojector CTAs skip the views whose cone misses their z range."""
+    torch = torch_cuda
+    PN = 24
+    zp = np.linspace(-10.0, 10.0, PN) if zpos else None
+    g = G.small(PN=PN, XN=10, YN=9, ZN=1200, dz=0.02, DNU=24, DNV=40, row_size=0.1, zpos=zp)
+    vol = phantom(g)
+    rng = np.random.default_rng(5)
+    prj = oracle.dd3_proj(g, vol).astype(np.float32) + 0.01 * rng.random(g.prj_shape).astype(np.float32)
+    ref_p = oracle.dd3_proj(g, vol)
+    ref_b = oracle.dd3_back(g, prj)
+    with cb.Plan(g, sat_mode=cb.CTLAB_SAT_ZPREFIX) as plan:
+        out_p = torch.zeros(g.prj_shape, dtype=torch.float32, device="cuda")
+        plan.proj(dev(torch, vol), out_p)
+        out_b = torch.zeros(g.vol_shape, dtype=torch.float32, device="cuda")
+        plan.back(dev(torch, prj), out_b)
+        torch.cuda.synchronize()
+        ep, eb = rel_l2(out_p.cpu().numpy(), ref_p), rel_l2(out_b.cpu().numpy(), ref_b)
+    record_error(f"proj/tall_z_{zpos}/zprefix", ep)
+    record_error(f"back/tall_z_{zpos}/zprefix", eb)
+    assert ep <= REL_L2 and eb <= REL_L2, (ep, eb)
