@@ -10,6 +10,7 @@ from ._lib import (CTLAB_ERR_CUDA, CTLAB_ERR_INTERNAL, CTLAB_ERR_INVALID_ARG, CT
 from .dd3 import (Batch, DD3Back_gpu, DD3Proj_gpu, Plan, back, ellipsoid_phantom, proj,
                   random_ellipsoids)
 from .geometry import DD3Geometry, config1, config2, config3, shepp_logan_ellipsoids, small
+from .multi import DistributedPlan, ViewSplit
 
 __all__ = [
     "CTLAB_OK", "CTLAB_ERR_INVALID_ARG", "CTLAB_ERR_UNSUPPORTED", "CTLAB_ERR_CUDA", "CTLAB_ERR_OOM",
@@ -17,5 +18,5 @@ __all__ = [
     "CtlabError",
     "load", "DD3Proj_gpu", "DD3Back_gpu", "Plan", "Batch", "proj", "back", "ellipsoid_phantom",
     "random_ellipsoids", "DD3Geometry", "config1", "config2", "config3", "small",
-    "shepp_logan_ellipsoids",
+    "shepp_logan_ellipsoids", "DistributedPlan", "ViewSplit",
 ]

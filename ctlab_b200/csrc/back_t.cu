@@ -30,6 +30,7 @@
 // the issue of view l+2's copy.  Views whose footprint exceeds a stage read P
 // from global memory.  Epilogue: in-plane mask and optionally the OS-SART
 // update x = (x + lambda * acc/colSum) * mask.
+#include <climits>
 #include <cmath>
 #include <type_traits>
 #include <utility>
@@ -135,7 +136,15 @@ __global__ void __launch_bounds__(kThreads, 1) dd3_back_t_kernel(BackArgs a, int
     const int cx = col & (kB - 1), cy = col / kB;
     const int x = bx0 + cx, y = by0 + cy;
     const int k0 = blockIdx.z * (kZS * KSEG) + zs * KSEG;
-    const int DNU = a.DNU, DNV = a.DNV, ZN = a.ZN, n = a.n;
+    const int DNU = a.DNU, DNV = a.DNV, ZN = a.ZN;
+    // the list positions this CTA visits: all, or (ZSKIP) the range of views
+    // whose cone can meet its z block
+    int lb = 0, n = a.n;
+    if (ZSKIP && a.zrange) {
+        const int2 r = a.zrange[blockIdx.z];
+        lb = r.x;
+        n = max(r.y - r.x, 0);
+    }
     const double dx = a.dx;
     const double x_lo = a.x_c0 - 0.5 * dx, y_lo = a.y_c0 - 0.5 * dx;
     const DetTable t = det_table_layout(DNU, DNV);
@@ -159,7 +168,7 @@ __global__ void __launch_bounds__(kThreads, 1) dd3_back_t_kernel(BackArgs a, int
     // and each column's z -> v map (warps 4-5)
     auto geometry = [&](int l) {
         if (l >= n) return;
-        const DevView &V = a.views[a.view_list[l]];
+        const DevView &V = a.views[a.view_list[lb + l]];
         const int sl = l % kGeo;
         if (tid < kB * (kB + 1)) {
             const int r = tid / (kB + 1), q = tid - r * (kB + 1);
@@ -213,7 +222,7 @@ __global__ void __launch_bounds__(kThreads, 1) dd3_back_t_kernel(BackArgs a, int
         s_rows[b] = meets ? (fits ? rows : 0) : -1; // -1: the view misses the brick
         mbar_arrive_expect_tx(&s_bar[b], fits ? (uint32_t)(4 * rows * vp) : 0u);
         if (fits)
-            bulk_copy_g2s(pbuf + (size_t)b * rmax * vp, Pall + l * pstride + (long long)lo * vp,
+            bulk_copy_g2s(pbuf + (size_t)b * rmax * vp, Pall + (long long)(lb + l) * pstride + (long long)lo * vp,
                           (uint32_t)(4 * rows * vp), &s_bar[b]);
     };
 
@@ -305,7 +314,7 @@ __global__ void __launch_bounds__(kThreads, 1) dd3_back_t_kernel(BackArgs a, int
                 }
             } else {
                 // footprint wider than a stage: P from global memory
-                const float *Pg = Pall + li * pstride;
+                const float *Pg = Pall + (long long)(lb + li) * pstride;
                 float2 *Ec = E + ac * es2;
                 auto eval = [&](int i) {
                     float e = fmaf(wb, __ldg(Pg + (size_t)ib * vp + i), wa * __ldg(Pg + (size_t)ia * vp + i));
@@ -411,6 +420,62 @@ size_t dyn_smem(int rmax, int vp, int es2)
     return 4 * 2 * (size_t)rmax * vp + sizeof(float2) * 2 * (size_t)kCols * es2;
 }
 
+// Per z block of zblk voxels (one CTA each): the first and one-past-last list
+// positions of the views whose cone can meet the block anywhere over the
+// volume's footprint.  A voxel at height z meets the detector when the ray's
+// detector z, S_z + t (z - S_z), lies within the rows; t = 1 / w with w the
+// point's distance from the source over the detector's, linear in the point,
+// so its extremes are at the footprint's corners.  One voxel of margin.
+__global__ void __launch_bounds__(256) zrange_kernel(BackArgs a, int zblk, int2 *out)
+{
+    __shared__ int s_lo[8], s_hi[8];
+    const int bz = blockIdx.x;
+    const double zb_lo = a.z_lo + (double)bz * zblk * a.dz - a.dz;
+    const double zb_hi = a.z_lo + (double)min((bz + 1) * zblk, a.ZN) * a.dz + a.dz;
+    const DetTable t = det_table_layout(a.DNU, a.DNV);
+    const double d_lo = fmin(a.det[t.off_bz], a.det[t.off_bz + a.DNV]);
+    const double d_hi = fmax(a.det[t.off_bz], a.det[t.off_bz + a.DNV]);
+    const double x0 = a.x_c0 - 0.5 * a.dx, x1 = x0 + a.XN * a.dx;
+    const double y0 = a.y_c0 - 0.5 * a.dx, y1 = y0 + a.YN * a.dx;
+    int lo = INT_MAX, hi = -1;
+    for (int l = threadIdx.x; l < a.n; l += blockDim.x) {
+        const DevView &V = a.views[a.view_list[l]];
+        const double den = cross2(V.B0x - V.Sx, V.B0y - V.Sy, V.Ex, V.Ey);
+        double wmin = 1e300, wmax = -1e300;
+        for (int c = 0; c < 4; ++c) {
+            const double px = (c & 1) ? x1 : x0, py = (c & 2) ? y1 : y0;
+            const double w = cross2(px - V.Sx, py - V.Sy, V.Ex, V.Ey) / den;
+            wmin = fmin(wmin, w);
+            wmax = fmax(wmax, w);
+        }
+        bool meets = true;
+        if (wmin > 0.0) {
+            const double e0 = d_lo + V.zP - V.Sz, e1 = d_hi + V.zP - V.Sz;
+            const double zlo = V.Sz + fmin(fmin(wmin * e0, wmax * e0), fmin(wmin * e1, wmax * e1));
+            const double zhi = V.Sz + fmax(fmax(wmin * e0, wmax * e0), fmax(wmin * e1, wmax * e1));
+            meets = zhi >= zb_lo && zlo <= zb_hi;
+        }
+        if (meets) {
+            lo = min(lo, l);
+            hi = max(hi, l);
+        }
+    }
+    lo = (int)__reduce_min_sync(0xffffffffu, (unsigned)lo);
+    hi = __reduce_max_sync(0xffffffffu, hi);
+    if ((threadIdx.x & 31) == 0) {
+        s_lo[threadIdx.x >> 5] = lo;
+        s_hi[threadIdx.x >> 5] = hi;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+            lo = min(lo, s_lo[w]);
+            hi = max(hi, s_hi[w]);
+        }
+        out[bz] = hi >= lo ? make_int2(lo, hi + 1) : make_int2(0, 0);
+    }
+}
+
 template <int KSEG, int VPT, bool ZSKIP>
 cudaError_t launch_k(const BackArgs &a, cudaStream_t s)
 {
@@ -420,6 +485,11 @@ cudaError_t launch_k(const BackArgs &a, cudaStream_t s)
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     dim3 grid((a.XN + kB - 1) / kB, (a.YN + kB - 1) / kB, (a.ZN + kZS * KSEG - 1) / (kZS * KSEG));
+    if (ZSKIP && a.zrange) {
+        zrange_kernel<<<grid.z, 256, 0, s>>>(a, kZS * KSEG, a.zrange);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
     kern<<<grid, kThreads, sm, s>>>(a, es2, a.rmax);
     return cudaGetLastError();
 }

@@ -289,6 +289,7 @@ struct BackArgs {
     int *err;             // device error word (bounded waits)
     const float *pv;      // projection v-prefixes [n][DNU][vp] (sat mode ZPREFIX)
     int zskip;            // a helical scan: views may miss a CTA's z range (tested, then skipped)
+    int2 *zrange;         // device scratch, one per z block: list positions [x, y) that can meet it
 };
 cudaError_t launch_back(const BackArgs &a, cudaStream_t s, int *launches);
 // Backprojector on projection v-prefixes (sat mode ZPREFIX).

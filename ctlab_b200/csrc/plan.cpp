@@ -72,7 +72,7 @@ void plan_free(ctlab_plan *p)
     DeviceGuard g(p->device);
     void *bufs[] = {p->d_views, p->d_det, p->d_all_views, p->d_list, p->d_sat_y, p->d_sat_x, p->d_zt_y, p->d_zt_x, p->d_pv,
                     p->d_q, p->d_ticket, p->d_flags, p->d_agg, p->d_pref, p->d_err,
-                    p->d_groups_all, p->d_groups_scratch};
+                    p->d_groups_all, p->d_groups_scratch, p->d_zrange};
     for (void *b : bufs)
         if (b) cudaFree(b);
     for (auto &e : p->ev)
@@ -248,6 +248,7 @@ int plan_back_list(ctlab_plan *p, const int *d_list, int n, const unsigned char 
     a.rmax = p->back_rmax;
     a.err = p->d_err;
     a.pv = p->d_pv;
+    a.zrange = p->d_zrange;
     for (const DevView &V : g.views)
         if (V.zP != g.views[0].zP) a.zskip = 1; // a helical scan
     if (n == 0 && epilogue == BACK_PLAIN) {
@@ -383,6 +384,7 @@ int ctlab_plan_create(const ctlab_geometry *geom, int device, int sat_mode, ctla
         chk(dmalloc((char **)&p->d_q, esz * (size_t)g.PN * (g.DNU + 1) * p->vp, bytes));
     else
         p->q_capacity = 0;
+    if (zpre) chk(dmalloc(&p->d_zrange, (size_t)g.ZN / 32 + 2, bytes)); // z blocks of >= 32 voxels
     // lookback state sized for the largest scan
     size_t tiles = 0, state = 0;
     auto need = [&](int planes, int ns, int nk, int chunk) {

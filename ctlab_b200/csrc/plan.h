@@ -26,6 +26,7 @@ struct ctlab_plan {
     int zp = 0;                 // z stride of the volume SATs
     void *d_q = nullptr; // projection SATs [q_capacity][DNU+1][vp]
     float *d_pv = nullptr; // projection v-prefixes [q_capacity][DNU][vp] (sat mode ZPREFIX)
+    int2 *d_zrange = nullptr; // backprojector view range per z block (sat mode ZPREFIX)
     int vp = 0;
     int q_capacity = 0;
     int proj_cmax = 2;  // projector staging columns
