@@ -503,6 +503,7 @@ def run_learned(args):
         losses.append(net.train_step(x2, x30, rng.integers(0, g.ZN, 8), SCALE, lr=max(lr, 2e-5)))
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
+    net.check_kernels()
 
     truth, meas = scan(7)
     clk = ClockSampler(local).__enter__()
@@ -518,6 +519,7 @@ def run_learned(args):
     t2 = event_ms(lambda: plan.os_sart(xl, meas, os_num=OS, iter_num=2))
     xw = torch.zeros_like(truth)
     tcnn = event_ms(lambda: net.predict_volume(xl, SCALE, xw))
+    net.check_kernels()
     rmse_warm = float(torch.sqrt(torch.mean((xw - truth) ** 2)))
     xc = xw.clone()
     res_cont = plan.os_sart(xc, meas, os_num=OS, iter_num=IT, residuals=True)

@@ -92,6 +92,7 @@ _SIGNATURES = {
                                  C.c_float, _fp, _vp]),
     "ctlab_cg": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int, _fp, _vp]),
     "ctlab_plan_autotune": (C.c_int, [_vp, _vp, _vp, C.c_char_p, _fp]),
+    "ctlab_cnn_check": (C.c_int, [_vp]),
     "ctlab_plan_proj_tiles": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "ctlab_batch_create": (C.c_int, [C.POINTER(_vp), C.c_int, C.POINTER(_vp)]),
     "ctlab_batch_destroy": (C.c_int, [_vp]),

@@ -7,16 +7,17 @@
 // centre channel plus the last convolution (a residual correction).
 // Channels are padded to 16 (input, last output) or 64.
 //
-//   conv3x3_kernel  implicit GEMM, M = pixels (an 8 x 16 tile per CTA), N =
-//                   output channels, K = 9 taps x input channels; the CTA
-//                   keeps the layer's weights in shared memory and loops over
-//                   tiles; the input halo tile and the weights use a 16-byte
-//                   XOR swizzle so ldmatrix reads are bank-conflict free;
-//                   mma.sync m16n8k16 BF16 -> FP32.  Epilogues: bias + ReLU
-//                   (forward), mask by an activation's sign (backward through
-//                   ReLU: the data gradient is the same convolution with the
-//                   weights flipped in space and transposed in channels), or
-//                   bias + centre channel in FP32 (the output layer).
+//   conv3x3_kernel  implicit GEMM on the 5th-generation tensor cores
+//                   (tcgen05): M = 128 output pixels (an 8 x 16 tile), N =
+//                   output channels, K = 9 taps x input channels, one
+//                   M128 x N x K16 MMA per (tap, 16 channels) with both
+//                   operands in shared memory and the FP32 accumulator in
+//                   tensor memory; the CTA keeps the layer's weights in
+//                   shared memory and loops over tiles.  Epilogues: bias +
+//                   ReLU, mask by an activation's sign (the data gradient =
+//                   the same convolution with the weights flipped in space
+//                   and transposed in channels), bias + centre channel in
+//                   FP32 (output layer).
 //   wgrad_kernel    dW[co][tap][ci] = sum_p dPre[p][co] act[p + tap][ci]: per
 //                   CTA one tap and a split of the pixels (the K of this GEMM),
 //                   A and B fragments by ldmatrix.trans from the NHWC tiles,
@@ -29,6 +30,7 @@
 #include <cstdint>
 
 #include "internal.h"
+#include "tma.cuh"
 
 namespace ctlab {
 
@@ -86,107 +88,240 @@ struct ConvArgs {
     int B, H, W, epi;
 };
 
-template <int CI, int CO>
-__global__ void __launch_bounds__(kCT) conv3x3_kernel(ConvArgs a)
+// ---- 5th-generation tensor cores (tcgen05): one M = 128 x N = CO x K = 16 MMA
+// per (tap, 16 input channels), operands in shared memory, FP32 accumulator
+// in tensor memory.  Shared-memory operand layout (K-major, no swizzle):
+// 16-byte chunks of 8 channels, the rows of a chunk plane 16 bytes apart,
+// groups of 8 rows SBO bytes apart, the two 8-channel halves of an MMA's K
+// LBO bytes apart.
+
+constexpr int kTPix = kTH * kTW;       // 128 output pixels: the MMA's M
+constexpr int kShift = kHH * kTW;      // 160 pixels of one column-shifted input tile (10 rows x 16)
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo)
 {
-    constexpr int NCH = CI / 8;  // 16-byte chunks per input pixel
-    constexpr int NT = CO / 8;   // n8 tiles
-    extern __shared__ __align__(128) unsigned char smem[];
-    bf16 *s_w = reinterpret_cast<bf16 *>(smem);               // [CO][9][CI] swizzled
-    bf16 *s_in = s_w + CO * 9 * CI;                           // [kHH*kHW][CI] swizzled
+    // start >> 4 in [0, 14), LBO >> 4 in [16, 30), SBO >> 4 in [32, 46),
+    // descriptor version 1 in [46, 48), no swizzle
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor, kind::f16: FP32 accumulator (bits 4-5 = 1), A and
+// B BF16 (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at 24.
+template <int N>
+constexpr uint32_t umma_idesc_bf16_m128()
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(kTPix >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                          uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t"
+        "}\n" ::"r"(tmem_d),
+        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate), "r"(0u));
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                 "%13, %14, %15}, [%16];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                   "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                   "=r"(v[15])
+                 : "r"(taddr));
+}
+
+__device__ int g_cnn_err; // a convolution's MMA wait ran out (read by ctlab_cnn_check)
+
+// 3x3 convolution, implicit GEMM on tcgen05: per tile of 8 x 16 output
+// pixels, M = 128 pixels, N = CO, K = 9 taps x CI.  The CTA keeps the layer's
+// weights in shared memory as [tap][chunk][co] and, per tile, three copies of
+// the input halo shifted by one column each, [dx][chunk][10 rows x 16]: the
+// A operand of tap (dy, dx) is then the 128 consecutive rows of copy dx from
+// row dy, a plain descriptor.  Thread 0 issues the 9 * CI/16 MMAs and
+// commits them to an mbarrier; the 4 warps read their 32 TMEM lanes (one
+// output pixel each, CO channels) and run the epilogue.  The global loads of
+// the next tile's halo are issued before the wait for this tile's MMAs.
+template <int CI, int CO>
+__global__ void __launch_bounds__(kCT, 1) conv3x3_kernel(ConvArgs a)
+{
+    constexpr int NCH = CI / 8;                 // 16-byte chunks per input pixel
+    constexpr int TCOLS = CO < 32 ? 32 : CO;    // TMEM columns (a power of 2 >= 32)
+    constexpr uint32_t kPlane = kShift * 16;    // bytes of one chunk plane of a shifted tile
+    constexpr uint32_t kIdesc = umma_idesc_bf16_m128<CO>();
+    constexpr int kHalo = kHH * kHW * NCH, kPer = (kHalo + kCT - 1) / kCT; // halo chunks, per thread
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char *s_w = smem;                          // [9][NCH][CO] chunks
+    unsigned char *s_a = smem + 9 * NCH * CO * 16;      // [3][NCH][kShift] chunks
+    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ uint32_t s_tmem;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
-    // the layer's weights, once per CTA
-    for (int i = tid; i < CO * 9 * NCH; i += kCT) {
-        const int c = i % NCH, rt = i / NCH; // rt = co*9 + tap
-        const int co = rt / 9;
-        const uint4 v = *reinterpret_cast<const uint4 *>(a.w + (size_t)rt * CI + c * 8);
-        *reinterpret_cast<uint4 *>(s_w + ((size_t)rt * NCH + swz<NCH>(co, c)) * 8) = v;
+    // the layer's weights, 12 loads in flight per thread
+    constexpr int kWChunks = CO * 9 * NCH;
+    for (int i0 = 0; i0 < kWChunks; i0 += 12 * kCT) {
+        uint4 v[12];
+#pragma unroll
+        for (int u = 0; u < 12; ++u) {
+            const int i = i0 + u * kCT + tid;
+            if (i < kWChunks) v[u] = *reinterpret_cast<const uint4 *>(a.w + (size_t)(i / NCH) * CI + (i % NCH) * 8);
+        }
+#pragma unroll
+        for (int u = 0; u < 12; ++u) {
+            const int i = i0 + u * kCT + tid;
+            if (i < kWChunks) {
+                const int kc = i % NCH, rt = i / NCH; // rt = co*9 + tap
+                const int co = rt / 9, t = rt - co * 9;
+                *reinterpret_cast<uint4 *>(s_w + ((size_t)(t * NCH + kc) * CO + co) * 16) = v[u];
+            }
+        }
     }
+    __syncwarp(); // the .sync.aligned tcgen05 instructions need converged warps
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&s_tmem)),
+                     "r"(TCOLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (tid == 0) {
+        mbar_init(&s_bar, 1);
+        mbar_fence_init();
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); // weights visible to the tensor cores
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    const uint32_t w_addr = smem_addr(s_w), a_addr = smem_addr(s_a);
+
     const int tiles_y = (a.H + kTH - 1) / kTH, tiles_x = (a.W + kTW - 1) / kTW;
     const int ntiles = a.B * tiles_y * tiles_x;
-    const uint32_t w_base = smem_u32(s_w), in_base = smem_u32(s_in);
+    // halo chunk i of tile `tile` into registers (zero outside the image)
+    uint4 hv[kPer];
+    auto load_halo = [&](int tile) {
+        const int b = tile / (tiles_y * tiles_x), tr = tile % (tiles_y * tiles_x);
+        const int y0 = (tr / tiles_x) * kTH, x0 = (tr % tiles_x) * kTW;
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+            const int i = u * kCT + tid;
+            const int q = i % (kHH * kHW), kc = i / (kHH * kHW);
+            const int row = q / kHW, col = q - row * kHW;
+            const int y = y0 - 1 + row, x = x0 - 1 + col;
+            hv[u] = make_uint4(0u, 0u, 0u, 0u);
+            if (tile < ntiles && i < kHalo && y >= 0 && y < a.H && x >= 0 && x < a.W)
+                hv[u] = *reinterpret_cast<const uint4 *>(a.in + (((size_t)b * a.H + y) * a.W + x) * CI + kc * 8);
+        }
+    };
+    // registers -> the three column-shifted tiles (halo column col -> column col - dx of copy dx)
+    auto store_halo = [&]() {
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) {
+            const int i = u * kCT + tid;
+            const int q = i % (kHH * kHW), kc = i / (kHH * kHW);
+            const int row = q / kHW, col = q - row * kHW;
+            if (i < kHalo) {
+#pragma unroll
+                for (int dx = 0; dx < 3; ++dx) {
+                    const int c = col - dx;
+                    if (c >= 0 && c < kTW)
+                        *reinterpret_cast<uint4 *>(s_a + (size_t)(dx * NCH + kc) * kPlane + (size_t)(row * kTW + c) * 16) =
+                            hv[u];
+                }
+            }
+        }
+        // generic-proxy stores visible to the tensor cores (async proxy)
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    };
 
+    uint32_t phase = 0;
+    bool ok = true;
+    load_halo(blockIdx.x);
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int b = tile / (tiles_y * tiles_x), tr = tile % (tiles_y * tiles_x);
         const int y0 = (tr / tiles_x) * kTH, x0 = (tr % tiles_x) * kTW;
-        __syncthreads(); // previous tile's reads of s_in done (and the weights stored)
-        for (int i = tid; i < kHH * kHW * NCH; i += kCT) {
-            const int c = i % NCH, q = i / NCH;
-            const int y = y0 - 1 + q / kHW, x = x0 - 1 + q % kHW;
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (y >= 0 && y < a.H && x >= 0 && x < a.W)
-                v = *reinterpret_cast<const uint4 *>(a.in + (((size_t)b * a.H + y) * a.W + x) * CI + c * 8);
-            *reinterpret_cast<uint4 *>(s_in + ((size_t)q * NCH + swz<NCH>(q, c)) * 8) = v;
-        }
+        store_halo();
         __syncthreads();
-
-        float acc[2][NT][4];
-#pragma unroll
-        for (int m = 0; m < 2; ++m)
-#pragma unroll
-            for (int n = 0; n < NT; ++n)
-#pragma unroll
-                for (int e = 0; e < 4; ++e) acc[m][n][e] = 0.f;
-
-        const int mi = lane >> 3, ri = lane & 7;
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll 1
-        for (int t = 0; t < 9; ++t) {
-            const int dy = t / 3, dx = t % 3;
+            for (int t = 0; t < 9; ++t) {
+                const int dy = t / 3, dx = t - dy * 3;
 #pragma unroll
-            for (int c16 = 0; c16 < CI / 16; ++c16) {
-                uint32_t af[2][4];
-#pragma unroll
-                for (int m = 0; m < 2; ++m) {
-                    const int r = warp * 2 + m; // tile row
-                    const int px = (mi & 1) * 8 + ri, ch = 2 * c16 + (mi >> 1);
-                    const int q = (r + dy) * kHW + px + dx;
-                    ldsm_x4(in_base + (uint32_t)((q * NCH + swz<NCH>(q, ch)) * 16), af[m][0], af[m][1], af[m][2],
-                            af[m][3]);
-                }
-#pragma unroll
-                for (int n2 = 0; n2 < NT / 2; ++n2) {
-                    const int co = n2 * 16 + (mi >> 1) * 8 + ri, ch = 2 * c16 + (mi & 1);
-                    uint32_t b0, b1, b2, b3;
-                    ldsm_x4(w_base + (uint32_t)(((co * 9 + t) * NCH + swz<NCH>(co, ch)) * 16), b0, b1, b2, b3);
-#pragma unroll
-                    for (int m = 0; m < 2; ++m) {
-                        mma_bf16(acc[m][2 * n2], af[m][0], af[m][1], af[m][2], af[m][3], b0, b1);
-                        mma_bf16(acc[m][2 * n2 + 1], af[m][0], af[m][1], af[m][2], af[m][3], b2, b3);
-                    }
+                for (int kk = 0; kk < CI / 16; ++kk) {
+                    const uint64_t ad = umma_desc(a_addr + (uint32_t)(dx * NCH + 2 * kk) * kPlane + (uint32_t)(dy * kTW) * 16,
+                                                  kPlane, 128);
+                    const uint64_t bd = umma_desc(w_addr + (uint32_t)((t * NCH + 2 * kk) * CO) * 16, CO * 16, 128);
+                    umma_bf16(tmem, ad, bd, kIdesc, (t | kk) != 0);
                 }
             }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_addr(&s_bar))
+                         : "memory");
         }
+        // the next tile's halo loads are in flight while the MMAs run
+        load_halo(tile + gridDim.x);
+        if (!mbar_wait(&s_bar, phase)) ok = false;
+        phase ^= 1u;
+        __syncwarp();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 
-        // epilogue: fragment (row lane/4 (+8), channels 2*(lane%4) + {0,1})
+        // accumulator row m = 32 warp + lane: output pixel (m / 16, m % 16)
+        uint32_t v[CO];
 #pragma unroll
-        for (int m = 0; m < 2; ++m) {
-            const int y = y0 + warp * 2 + m;
+        for (int j = 0; j < CO / 16; ++j) {
+            uint32_t r16[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(j * 16), r16);
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int x = x0 + (lane >> 2) + 8 * h;
-                if (y >= a.H || x >= a.W) continue;
-                const size_t pix = ((size_t)b * a.H + y) * a.W + x;
+            for (int e = 0; e < 16; ++e) v[j * 16 + e] = r16[e];
+        }
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        const int m = warp * 32 + lane;
+        const int y = y0 + m / kTW, x = x0 + m % kTW;
+        if (ok && y < a.H && x < a.W) {
+            const size_t pix = ((size_t)b * a.H + y) * a.W + x;
+            if (a.epi == CTLAB_CNN_EPI_RESIDUAL) {
+                a.out_f32[pix] = __uint_as_float(v[0]) + a.bias[0] + a.center[pix];
+            } else {
+                uint4 mk[CO / 8];
+                if (a.epi == CTLAB_CNN_EPI_MASK) {
 #pragma unroll
-                for (int n = 0; n < NT; ++n) {
-                    const int co = n * 8 + 2 * (lane & 3);
-                    float v0 = acc[m][n][2 * h], v1 = acc[m][n][2 * h + 1];
-                    if (a.epi == CTLAB_CNN_EPI_RESIDUAL) {
-                        if (co == 0) a.out_f32[pix] = v0 + a.bias[0] + a.center[pix];
-                        continue;
-                    }
+                    for (int c8 = 0; c8 < CO / 8; ++c8) mk[c8] = *reinterpret_cast<const uint4 *>(a.mask + pix * CO + c8 * 8);
+                }
+#pragma unroll
+                for (int c8 = 0; c8 < CO / 8; ++c8) {
+                    float f[8];
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) f[e] = __uint_as_float(v[c8 * 8 + e]);
                     if (a.epi == CTLAB_CNN_EPI_RELU) {
-                        v0 = fmaxf(v0 + a.bias[co], 0.f);
-                        v1 = fmaxf(v1 + a.bias[co + 1], 0.f);
+#pragma unroll
+                        for (int e = 0; e < 8; ++e) f[e] = fmaxf(f[e] + a.bias[c8 * 8 + e], 0.f);
                     } else if (a.epi == CTLAB_CNN_EPI_MASK) {
-                        const __nv_bfloat162 mk = *reinterpret_cast<const __nv_bfloat162 *>(a.mask + pix * CO + co);
-                        if (!(__bfloat162float(mk.x) > 0.f)) v0 = 0.f;
-                        if (!(__bfloat162float(mk.y) > 0.f)) v1 = 0.f;
+                        const __nv_bfloat16 *mb = reinterpret_cast<const __nv_bfloat16 *>(&mk[c8]);
+#pragma unroll
+                        for (int e = 0; e < 8; ++e)
+                            if (!(__bfloat162float(mb[e]) > 0.f)) f[e] = 0.f;
                     }
-                    *reinterpret_cast<__nv_bfloat162 *>(a.out + pix * CO + co) = __floats2bfloat162_rn(v0, v1);
+                    uint4 o;
+                    __nv_bfloat162 *ob = reinterpret_cast<__nv_bfloat162 *>(&o);
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) ob[e] = __floats2bfloat162_rn(f[2 * e], f[2 * e + 1]);
+                    *reinterpret_cast<uint4 *>(a.out + pix * CO + c8 * 8) = o;
                 }
             }
         }
+        // TMEM and the shifted tiles are free for the next tile
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+    }
+    if (!ok) atomicExch(&g_cnn_err, 1);
+    __syncwarp();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCOLS));
     }
 }
 
@@ -391,12 +526,19 @@ unsigned grid_n(long long n, int bs)
 template <int CI, int CO>
 cudaError_t conv_launch(const ConvArgs &a, cudaStream_t s)
 {
-    const size_t sm = sizeof(bf16) * ((size_t)CO * 9 * CI + (size_t)kHH * kHW * CI);
+    const size_t sm = 16 * ((size_t)9 * (CI / 8) * CO + (size_t)3 * (CI / 8) * kShift);
     auto k = conv3x3_kernel<CI, CO>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kCT, sm);
+    if (e != cudaSuccess) return e;
+    // resident CTAs each hold max(CO, 32) of the SM's 512 TMEM columns
+    per_sm = std::max(1, std::min(per_sm, 512 / std::max(CO, 32)));
     const long long ntiles = (long long)a.B * ((a.H + kTH - 1) / kTH) * ((a.W + kTW - 1) / kTW);
-    const unsigned grid = (unsigned)std::min<long long>(ntiles, 148LL * 2 * 4);
+    const unsigned grid = (unsigned)std::min<long long>(ntiles, (long long)sms * per_sm);
     k<<<grid, kCT, sm, s>>>(a);
     return cudaGetLastError();
 }
@@ -501,6 +643,20 @@ int ctlab_cnn_adam(float *d_w, float *d_m, float *d_v, float *d_g, int co, int c
                                                                     c2, (bf16 *)d_wf, (bf16 *)d_wt);
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? set_status(CTLAB_OK, "") : cuda_status(e, "Adam");
+}
+
+int ctlab_cnn_check(void *stream)
+{
+    cudaStream_t s = (cudaStream_t)stream;
+    int err = 0;
+    CTLAB_CUDA_TRY(cudaMemcpyFromSymbolAsync(&err, g_cnn_err, sizeof(int), 0, cudaMemcpyDeviceToHost, s));
+    CTLAB_CUDA_TRY(cudaStreamSynchronize(s));
+    if (err) {
+        const int zero = 0;
+        CTLAB_CUDA_TRY(cudaMemcpyToSymbol(g_cnn_err, &zero, sizeof(int)));
+        return set_status(CTLAB_ERR_TIMEOUT, "a convolution's tensor-core wait ran out");
+    }
+    return set_status(CTLAB_OK, "");
 }
 
 } // extern "C"

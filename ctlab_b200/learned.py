@@ -133,6 +133,11 @@ class WarmStartNet:
         self.step(lr)
         return loss
 
+    def check_kernels(self):
+        """Raises if a convolution gave up waiting for its tensor-core MMAs
+        since the last check (synchronises the current stream)."""
+        check(self.lib.ctlab_cnn_check(None))
+
     def predict_volume(self, vol_in, scale, out, batch: int = 16):
         """Runs the network over every z slice of vol_in into out (both [YN][XN][ZN])."""
         torch = self.torch

@@ -288,13 +288,19 @@ int ctlab_batch_proj(ctlab_batch *batch, const float *const *d_vols, const unsig
 
 /* 3x3 convolution, stride 1, zero padding, on NHWC BF16 tensors
  * d_in [B][H][W][ci] with weights d_w [co][9][ci] (tap = 3*dy + dx), FP32
- * accumulation on the tensor cores.  (ci, co) is (16, 64), (64, 64) or
+ * accumulation on the 5th-generation tensor cores (tcgen05, TMEM
+ * accumulator).  (ci, co) is (16, 64), (64, 64) or
  * (64, 16).  The data gradient of a layer is this convolution with the
  * flipped, channel-transposed weights (ctlab_cnn_adam writes them) and the
  * MASK epilogue. */
 int ctlab_cnn_conv(const void *d_in, int ci, const void *d_w, const float *d_bias, int co, int B, int H, int W,
                    int epi, void *d_out, const void *d_mask, float *d_out_f32, const float *d_center,
                    void *stream);
+
+/* Synchronises the stream and reports whether a convolution since the last
+ * check gave up waiting for its tensor-core MMAs (CTLAB_ERR_TIMEOUT; its
+ * outputs are then invalid).  Clears the flag. */
+int ctlab_cnn_check(void *stream);
 
 /* Weight (and, with d_db, bias) gradients of a convolution, accumulated:
  * d_dw [co][9][ci] += sum_p dpre[p][co] * act[p + tap][ci]. */

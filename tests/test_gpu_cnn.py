@@ -55,6 +55,7 @@ def test_conv_forward_matches_numpy(torch_cuda, ci, co, shape):
         out = torch.zeros((B, H, W), dtype=torch.float32, device="cuda")
         assert lib.ctlab_cnn_conv(dx.data_ptr(), ci, dw.data_ptr(), db.data_ptr(), co, B, H, W, 2, None, None,
                                   out.data_ptr(), center.data_ptr(), None) == 0
+        assert lib.ctlab_cnn_check(None) == 0  # no tensor-core wait ran out
         got = out.cpu().numpy()
         want = ref[..., 0] + center.cpu().numpy()
         assert rel(got, want) <= 1e-5
@@ -62,6 +63,7 @@ def test_conv_forward_matches_numpy(torch_cuda, ci, co, shape):
         out = torch.zeros((B, H, W, co), dtype=torch.bfloat16, device="cuda")
         assert lib.ctlab_cnn_conv(dx.data_ptr(), ci, dw.data_ptr(), db.data_ptr(), co, B, H, W, 0, out.data_ptr(),
                                   None, None, None, None) == 0
+        assert lib.ctlab_cnn_check(None) == 0
         got = from_bf16_dev(out).reshape(B, H, W, co)
         want = np.maximum(ref, 0)
         assert rel(got, want) <= 6e-3  # BF16 output rounding (2^-9 relative)
