@@ -346,7 +346,9 @@ def run_ours(args):
             "e2e": e2e,
             "gpu_launches": launches_per_step * args.steps,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                         "frac": achieved / peak,
+                         "peak_source": ("measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                                         else "fallback (6.65 TB/s, earlier measurement on this pool; no MEASURED_PEAKS.json)"),
                          "traffic": traffic, "algorithmic_bytes_per_launch": alg,
                          "launch_ms": t_dom},
             "kernels_ms": {"proj_sat": float(np.mean(proj_sat)), "proj": t_proj,
