@@ -77,6 +77,7 @@ void plan_free(ctlab_plan *p)
         if (b) cudaFree(b);
     for (auto &e : p->ev)
         if (e) cudaEventDestroy(e);
+    sart_work_free(p->sart);
     delete p;
 }
 

@@ -6,6 +6,10 @@
 
 #include "internal.h"
 
+namespace ctlab {
+struct SartWork; // OS-SART workspace and weights kept between calls (recon.cpp)
+}
+
 struct ctlab_plan {
     int device = 0;
     int sat_mode = CTLAB_SAT_FP64;
@@ -42,6 +46,7 @@ struct ctlab_plan {
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
     int last_launches = 0;
     long long bytes = 0;
+    ctlab::SartWork *sart = nullptr;
     std::mutex mu;
 };
 
@@ -54,6 +59,7 @@ struct GroupTab {
 };
 
 void plan_free(ctlab_plan *p);
+void sart_work_free(SartWork *w);
 // Groups the host list (positions into a device view list) and uploads the
 // table to d_dst (capacity cap ints); synchronous.
 int plan_groups(ctlab_plan *p, const std::vector<int> &host_list, int *d_dst, int cap, GroupTab &out,

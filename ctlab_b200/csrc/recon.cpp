@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstring>
 #include <initializer_list>
+#include <new>
 #include <utility>
 #include <vector>
 
@@ -58,6 +59,73 @@ int exact_residual(ctlab_plan *p, const float *d_x, const unsigned char *d_mask,
 
 } // namespace
 
+namespace ctlab {
+
+// OS-SART state kept on a plan between ctlab_os_sart calls: the buffers (so
+// repeated solves allocate nothing) and the view order, group tables and
+// SART weights (rowSum = A 1, colSum_s = B_s 1) of the last subsets and mask
+// used, identified by a hash of os_num, the order and the mask bytes.
+struct SartWork {
+    unsigned long long key = 0;
+    bool weights = false; // rows / cols hold the weights of `key`
+    std::vector<GroupTab> gtab;
+    struct Buf {
+        void *p = nullptr;
+        size_t cap = 0;
+    } order, groups, bsub, rows, cols, r, ones, acc, est;
+    ~SartWork()
+    {
+        for (Buf *b : {&order, &groups, &bsub, &rows, &cols, &r, &ones, &acc, &est})
+            if (b->p) cudaFree(b->p);
+    }
+};
+
+void sart_work_free(SartWork *w) { delete w; }
+
+} // namespace ctlab
+
+namespace {
+
+// Grows b to at least `bytes`; reports whether it was reallocated.
+int reserve(SartWork::Buf &b, size_t bytes, bool *moved)
+{
+    if (bytes <= b.cap && b.p) return CTLAB_OK;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    cudaError_t e = cudaMalloc(&b.p, bytes ? bytes : 1);
+    if (e != cudaSuccess) return cuda_status(e, "reconstruction workspace");
+    b.cap = bytes;
+    if (moved) *moved = true;
+    return CTLAB_OK;
+}
+
+unsigned long long sart_key(const ctlab_plan *p, int os_num, const std::vector<int> &order,
+                            const std::vector<unsigned char> &mask, bool has_mask)
+{
+    unsigned long long h = 1469598103934665603ull;
+    auto add = [&](const void *q, size_t n) {
+        const unsigned char *b = (const unsigned char *)q;
+        for (size_t i = 0; i < n; ++i) {
+            h ^= b[i];
+            h *= 1099511628211ull;
+        }
+    };
+    add(&os_num, sizeof os_num);
+    // the projector staging the group tables were planned with (the autotuner may change it)
+    for (const ProjTStaging *st : {&p->tst, &p->tst1}) {
+        const int f[8] = {st->G, st->NR, st->RB, st->ZS, st->CB, st->KB, st->nstage, (int)st->ok};
+        add(f, sizeof f);
+    }
+    add(order.data(), sizeof(int) * order.size());
+    const unsigned char m = has_mask;
+    add(&m, 1);
+    add(mask.data(), mask.size());
+    return h;
+}
+
+} // namespace
+
 extern "C" {
 
 int ctlab_os_sart(ctlab_plan *plan, float *d_x, const float *d_meas, const unsigned char *d_mask, int os_num,
@@ -101,63 +169,86 @@ int ctlab_os_sart(ctlab_plan *plan, float *d_x, const float *d_meas, const unsig
 
     const long long nd = (long long)g.DNU * g.DNV;
     const long long nv = (long long)g.XN * g.YN * g.ZN;
-    DevBuf d_order, d_bsub, d_rows, d_cols, d_r, d_ones, d_acc, d_est, d_groups;
     const int gcap = plan->groups_cap;
-    int rc = alloc(d_order, sizeof(int) * g.PN);
-    if (rc == CTLAB_OK) rc = alloc(d_groups, sizeof(int) * (size_t)gcap * (os_num + 1));
-    if (rc == CTLAB_OK) rc = alloc(d_bsub, sizeof(float) * nd * g.PN);
-    if (rc == CTLAB_OK) rc = alloc(d_rows, sizeof(float) * nd * g.PN);
-    if (rc == CTLAB_OK) rc = alloc(d_cols, sizeof(float) * nv * os_num);
-    if (rc == CTLAB_OK) rc = alloc(d_r, sizeof(float) * nd * nmax);
-    if (rc == CTLAB_OK) rc = alloc(d_ones, sizeof(float) * std::max(nd * nmax, nv));
-    if (rc == CTLAB_OK) rc = alloc(d_acc, sizeof(double) * 2);
-    if (rc == CTLAB_OK && h_resid) rc = alloc(d_est, sizeof(float) * nd * g.PN);
-    if (rc != CTLAB_OK) return rc;
-    CTLAB_CUDA_TRY(cudaMemcpyAsync(d_order.p, order.data(), sizeof(int) * g.PN, cudaMemcpyHostToDevice, s));
-    CTLAB_CUDA_TRY(launch_gather_views(d_meas, d_order.as<int>(), g.PN, nd, d_bsub.as<float>(), s));
-    // projector view groups: the whole order, then each subset
-    std::vector<GroupTab> gtab(os_num + 1);
-    rc = plan_groups(plan, order, d_groups.as<int>() + (size_t)gcap * os_num, gcap, gtab[os_num], s);
-    for (int k = 0; k < os_num && rc == CTLAB_OK; ++k) {
-        std::vector<int> sub(order.begin() + off[k], order.begin() + off[k + 1]);
-        rc = plan_groups(plan, sub, d_groups.as<int>() + (size_t)gcap * k, gcap, gtab[k], s);
+    // the mask's bytes identify the weights (a caller may rewrite a mask in place)
+    std::vector<unsigned char> hmask;
+    if (d_mask) {
+        hmask.resize((size_t)g.XN * g.YN);
+        CTLAB_CUDA_TRY(cudaMemcpyAsync(hmask.data(), d_mask, hmask.size(), cudaMemcpyDeviceToHost, s));
+        CTLAB_CUDA_TRY(cudaStreamSynchronize(s));
     }
-    if (rc != CTLAB_OK) return rc;
-
-    // rowSum = A 1 (masked volume of ones), colSum_s = B_s 1
-    CTLAB_CUDA_TRY(launch_fill(d_ones.as<float>(), 1.f, std::max(nd * nmax, nv), s));
-    rc = plan_volume_sat(plan, d_ones.as<float>(), d_mask, s);
-    if (rc == CTLAB_OK)
-        rc = plan_proj_list(plan, d_order.as<int>(), g.PN, gtab[os_num], d_rows.as<float>(), s, PROJ_PLAIN, nullptr,
-                            nullptr, nullptr);
-    for (int k = 0; k < os_num && rc == CTLAB_OK; ++k) {
-        const int n = off[k + 1] - off[k];
-        const int *lst = d_order.as<int>() + off[k];
-        rc = plan_proj_sat(plan, lst, n, d_ones.as<float>(), s);
+    const unsigned long long key = sart_key(plan, os_num, order, hmask, d_mask != nullptr);
+    if (!plan->sart) {
+        plan->sart = new (std::nothrow) SartWork();
+        if (!plan->sart) return set_status(CTLAB_ERR_OOM, "host allocation failed");
+    }
+    SartWork &W = *plan->sart;
+    bool moved = false;
+    int rc = reserve(W.order, sizeof(int) * g.PN, &moved);
+    if (rc == CTLAB_OK) rc = reserve(W.groups, sizeof(int) * (size_t)gcap * (os_num + 1), &moved);
+    if (rc == CTLAB_OK) rc = reserve(W.rows, sizeof(float) * nd * g.PN, &moved);
+    if (rc == CTLAB_OK) rc = reserve(W.cols, sizeof(float) * nv * os_num, &moved);
+    if (rc == CTLAB_OK) rc = reserve(W.bsub, sizeof(float) * nd * g.PN, nullptr);
+    if (rc == CTLAB_OK) rc = reserve(W.r, sizeof(float) * nd * nmax, nullptr);
+    if (rc == CTLAB_OK) rc = reserve(W.ones, sizeof(float) * std::max(nd * nmax, nv), nullptr);
+    if (rc == CTLAB_OK) rc = reserve(W.acc, sizeof(double) * 2, nullptr);
+    if (rc == CTLAB_OK && h_resid) rc = reserve(W.est, sizeof(float) * nd * g.PN, nullptr);
+    if (rc != CTLAB_OK) {
+        W.weights = false;
+        return rc;
+    }
+    int *d_order = (int *)W.order.p, *d_groups = (int *)W.groups.p;
+    float *d_bsub = (float *)W.bsub.p, *d_rows = (float *)W.rows.p, *d_cols = (float *)W.cols.p;
+    float *d_r = (float *)W.r.p, *d_ones = (float *)W.ones.p, *d_est = (float *)W.est.p;
+    double *d_acc = (double *)W.acc.p;
+    std::vector<GroupTab> &gtab = W.gtab;
+    if (moved || !W.weights || W.key != key) {
+        W.weights = false;
+        CTLAB_CUDA_TRY(cudaMemcpyAsync(d_order, order.data(), sizeof(int) * g.PN, cudaMemcpyHostToDevice, s));
+        // projector view groups: the whole order, then each subset
+        gtab.assign(os_num + 1, GroupTab());
+        rc = plan_groups(plan, order, d_groups + (size_t)gcap * os_num, gcap, gtab[os_num], s);
+        for (int k = 0; k < os_num && rc == CTLAB_OK; ++k) {
+            std::vector<int> sub(order.begin() + off[k], order.begin() + off[k + 1]);
+            rc = plan_groups(plan, sub, d_groups + (size_t)gcap * k, gcap, gtab[k], s);
+        }
+        if (rc != CTLAB_OK) return rc;
+        // rowSum = A 1 (masked volume of ones), colSum_s = B_s 1
+        CTLAB_CUDA_TRY(launch_fill(d_ones, 1.f, std::max(nd * nmax, nv), s));
+        rc = plan_volume_sat(plan, d_ones, d_mask, s);
         if (rc == CTLAB_OK)
-            rc = plan_back_list(plan, lst, n, d_mask, d_cols.as<float>() + nv * k, s, BACK_PLAIN, nullptr, 1.f, 0,
-                                0.f, 0.f);
+            rc = plan_proj_list(plan, d_order, g.PN, gtab[os_num], d_rows, s, PROJ_PLAIN, nullptr, nullptr, nullptr);
+        for (int k = 0; k < os_num && rc == CTLAB_OK; ++k) {
+            const int n = off[k + 1] - off[k];
+            const int *lst = d_order + off[k];
+            rc = plan_proj_sat(plan, lst, n, d_ones, s);
+            if (rc == CTLAB_OK)
+                rc = plan_back_list(plan, lst, n, d_mask, d_cols + nv * k, s, BACK_PLAIN, nullptr, 1.f, 0, 0.f, 0.f);
+        }
+        if (rc != CTLAB_OK) return rc;
+        W.key = key;
+        W.weights = true;
     }
-    if (rc != CTLAB_OK) return rc;
+    CTLAB_CUDA_TRY(launch_gather_views(d_meas, d_order, g.PN, nd, d_bsub, s));
 
     for (int it = 0; it < iter_num; ++it) {
         for (int k = 0; k < os_num; ++k) {
             const int n = off[k + 1] - off[k];
             if (n == 0) continue;
-            const int *lst = d_order.as<int>() + off[k];
+            const int *lst = d_order + off[k];
             rc = plan_volume_sat(plan, d_x, d_mask, s);
             if (rc == CTLAB_OK)
-                rc = plan_proj_list(plan, lst, n, gtab[k], d_r.as<float>(), s, PROJ_SART_RESIDUAL,
-                                    d_bsub.as<float>() + nd * off[k], d_rows.as<float>() + nd * off[k], nullptr);
-            if (rc == CTLAB_OK) rc = plan_proj_sat(plan, lst, n, d_r.as<float>(), s);
+                rc = plan_proj_list(plan, lst, n, gtab[k], d_r, s, PROJ_SART_RESIDUAL,
+                                    d_bsub + nd * off[k], d_rows + nd * off[k], nullptr);
+            if (rc == CTLAB_OK) rc = plan_proj_sat(plan, lst, n, d_r, s);
             if (rc == CTLAB_OK)
-                rc = plan_back_list(plan, lst, n, d_mask, d_x, s, BACK_SART_UPDATE, d_cols.as<float>() + nv * k,
+                rc = plan_back_list(plan, lst, n, d_mask, d_x, s, BACK_SART_UPDATE, d_cols + nv * k,
                                     lambda, clamp, min_v, max_v);
             if (rc != CTLAB_OK) return rc;
         }
         if (h_resid) {
-            rc = exact_residual(plan, d_x, d_mask, d_order.as<int>(), gtab[os_num], d_bsub.as<float>(),
-                                d_est.as<float>(), d_acc.as<double>(), s, h_resid + it);
+            rc = exact_residual(plan, d_x, d_mask, d_order, gtab[os_num], d_bsub,
+                                d_est, d_acc, s, h_resid + it);
             if (rc != CTLAB_OK) return rc;
         }
     }

@@ -193,7 +193,10 @@ int ctlab_plan_last_launches(const ctlab_plan *plan);
  *   x = (x + lambda * (B_s r)/colSum_s) * mask  (0 where colSum_s <= 1e-7)
  * optionally clamped to [min_v, max_v] when clamp != 0.  If h_resid is not
  * NULL it receives iter_num values ||b - A x_k|| / ||b|| after each
- * iteration.  Replaces the GPU body of OS_SART, src/DD3_GPU_recon.h:60-65. */
+ * iteration.  The plan keeps the call's workspace and SART weights; a later
+ * call with the same subsets, order and mask bytes reuses them without
+ * allocating (the mask is read back to the host to compare it).  Replaces the
+ * GPU body of OS_SART, src/DD3_GPU_recon.h:60-65. */
 int ctlab_os_sart(ctlab_plan *plan, float *d_x, const float *d_meas, const unsigned char *d_mask,
                   int os_num, int iter_num, float lambda, const int *h_order, int clamp,
                   float min_v, float max_v, float *h_resid, void *stream);

@@ -209,3 +209,43 @@ def test_reference_signature_cxx_entry_points_equal_device_path(torch_cuda, solv
         ref = x.cpu().numpy()
     err = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
     assert err <= 1e-6, err
+
+
+def test_os_sart_calls_reuse_weights_only_for_the_same_subsets_and_mask(torch_cuda):
+    """A plan keeps its OS-SART workspace and SART weights between calls: 2 + 2
+    iterations equal 4 in one call bit for bit; a mask rewritten in place, other
+    subsets or another order between calls give what a fresh plan gives."""
+    torch = torch_cuda
+    g, truth, prj = scan(2)
+    meas = dev(torch, prj)
+    mask_a = np.ones(g.XN * g.YN, np.uint8)
+    mask_b = (np.random.default_rng(9).random(g.XN * g.YN) > 0.25).astype(np.uint8)
+    with cb.Plan(g) as plan:
+        one = torch.zeros(g.vol_shape, dtype=torch.float32, device="cuda")
+        plan.os_sart(one, meas, dev(torch, mask_a), os_num=4, iter_num=4)
+        two = torch.zeros_like(one)
+        m = dev(torch, mask_a)
+        plan.os_sart(two, meas, m, os_num=4, iter_num=2)
+        plan.os_sart(two, meas, m, os_num=4, iter_num=2)
+        torch.cuda.synchronize()
+        assert torch.equal(one, two)
+        # same device buffer, new mask bytes
+        m.copy_(dev(torch, mask_b))
+        x_b = torch.zeros_like(one)
+        plan.os_sart(x_b, meas, m, os_num=4, iter_num=2)
+        # other subsets, then a custom order
+        x_c = torch.zeros_like(one)
+        plan.os_sart(x_c, meas, m, os_num=3, iter_num=2)
+        order = np.random.default_rng(1).permutation(g.PN)
+        x_d = torch.zeros_like(one)
+        plan.os_sart(x_d, meas, m, os_num=3, iter_num=2, order=order)
+        torch.cuda.synchronize()
+    with cb.Plan(g) as fresh:
+        refs = []
+        for os_num, o in ((4, None), (3, None), (3, order)):
+            x = torch.zeros_like(one)
+            fresh.os_sart(x, meas, dev(torch, mask_b), os_num=os_num, iter_num=2, order=o)
+            refs.append(x)
+        torch.cuda.synchronize()
+    for got, want in zip((x_b, x_c, x_d), refs):
+        assert torch.equal(got, want)
