@@ -188,8 +188,9 @@ def run_reference(args):
     prj_all = np.zeros(g.prj_shape, np.float32)
     prj_all[:2] = prj
     nviews = max(1, args.cpu_views // 2)
-    for _ in range(args.warmup if args.warmup < 2 else 1):
-        pass
+    # untimed warm-up: one short sample (thread pool start-up, page faults)
+    if args.warmup > 0:
+        cpu_sample(g, vol, prj_all, 1)
     vals = []
     for _ in range(max(1, args.steps)):
         vals.append(cpu_sample(g, vol, prj_all, nviews)["value"])
