@@ -58,9 +58,18 @@ struct ctlab_batch {
     cudaGraphExec_t gexec = nullptr;
     std::vector<const void *> graph_ptrs; // buffers the graph was captured with
     long long voxel_views = 0;
+    std::vector<std::vector<int>> staging; // each plan's projector staging when the items were made
 };
 
 namespace {
+
+// The fields of a plan's projector staging and view grouping that the work
+// items and launch row counts were derived from.
+std::vector<int> staging_sig(const ctlab_plan *p)
+{
+    const ProjTStaging &st = p->tst;
+    return {st.G, st.NR, st.RB, st.ZS, st.CB, st.KB, st.KR, st.nstage, p->groups_all_n, p->groups_all_G};
+}
 
 // Fills a case's projector arguments for all views of its plan (the
 // projection goes to d_prj); mirrors plan_proj_list's ZPREFIX branch.
@@ -309,6 +318,7 @@ int ctlab_batch_create(ctlab_plan *const *plans, int n, ctlab_batch **out)
         L->smem = std::max(L->smem, proj_t_smem_bytes(p->tst));
         for (double x : case_cost[i]) L->cost += x;
         b->voxel_views += (long long)p->g.XN * p->g.YN * p->g.ZN * p->g.PN;
+        b->staging.push_back(staging_sig(p));
     }
     std::stable_sort(b->launches.begin(), b->launches.end(),
                      [](const BatchLaunch &x, const BatchLaunch &y) { return x.cost > y.cost; });
@@ -408,6 +418,11 @@ int ctlab_batch_proj(ctlab_batch *b, const float *const *d_vols, const unsigned 
     const int n = (int)b->plans.size();
     for (int i = 0; i < n; ++i)
         if (!d_vols[i] || !d_prjs[i]) return set_status(CTLAB_ERR_INVALID_ARG, "null volume or projection buffer");
+    for (int i = 0; i < n; ++i)
+        if (staging_sig(b->plans[i]) != b->staging[i])
+            return set_status(CTLAB_ERR_INVALID_ARG,
+                              "a plan's projector staging changed (autotuned?) after the batch was created; "
+                              "create the batch again");
     DeviceGuard dg(b->device);
     cudaStream_t s = (cudaStream_t)stream;
     // launch parameters: every case's arguments with its output buffer

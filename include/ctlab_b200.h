@@ -264,7 +264,10 @@ int ctlab_plan_autotune(ctlab_plan *plan, const float *d_vol, float *d_prj, cons
  * a projection of all views. */
 int ctlab_plan_proj_tiles(const ctlab_plan *plan, int *tiles);
 
-/* A batch projects the scans of n z-prefix plans (one device) together. */
+/* A batch projects the scans of n z-prefix plans (one device) together.  The
+ * plans must outlive the batch; tune them (ctlab_plan_autotune) before
+ * creating it: a batch whose plans were re-staged afterwards refuses to run
+ * (CTLAB_ERR_INVALID_ARG). */
 typedef struct ctlab_batch ctlab_batch;
 int ctlab_batch_create(ctlab_plan *const *plans, int n, ctlab_batch **out);
 int ctlab_batch_destroy(ctlab_batch *batch);
