@@ -1,7 +1,7 @@
 """CUDA path (through the C ABI) against the FP64 CPU oracle.
 
-Bar: relative L2 <= 1e-4 for projection and backprojection (the target the
-north-star sets for FP32 outputs against an FP64 oracle); FP64 SATs to 1e-12
+Bar: relative L2 <= 1e-4 for projection and backprojection (the parity bar for
+FP32 outputs against an FP64 oracle); FP64 SATs to 1e-12
 relative.  Sizes are chosen so the oracle finishes in seconds.
 """
 import math
