@@ -677,25 +677,35 @@ std::vector<std::vector<int>> as_views(std::vector<std::vector<int>> groups, con
 int t_zrows(const HostGeometry &g, const std::vector<std::vector<int>> &groups, int rows, int zs)
 {
     int need = 4;
+    std::vector<double> emins, emaxs; // per (row block, view of the group)
     for (const auto &grp : groups) {
         const DevView &V0 = g.views[grp[0]];
         const int jstep = std::max(1, V0.na / 64);
+        // z-boundary extremes of each row block per view (independent of tile and slice)
+        emins.assign((size_t)zs * grp.size(), 1e300);
+        emaxs.assign((size_t)zs * grp.size(), -1e300);
+        for (int zb = 0; zb < zs; ++zb) {
+            const int w0 = zb * rows, w1 = std::min(g.DNV, w0 + rows);
+            for (size_t q = 0; q < grp.size(); ++q) {
+                const DevView &V = g.views[grp[q]];
+                double &mn = emins[zb * grp.size() + q], &mx = emaxs[zb * grp.size() + q];
+                for (int w = w0; w <= w1; ++w) {
+                    const double e = (g.bz[w] + V.zP - V.Sz) / g.dz;
+                    mn = std::min(mn, e);
+                    mx = std::max(mx, e);
+                }
+            }
+        }
         for (int u0 = 0; u0 < g.DNU; u0 += kTU) {
             const int nu = std::min(kTU, g.DNU - u0);
             const int us[3] = {u0, u0 + nu / 2, u0 + nu - 1};
             for (int zb = 0; zb < zs; ++zb) {
-                const int w0 = zb * rows, w1 = std::min(g.DNV, w0 + rows);
                 for (int j = 0; j < V0.na; j += (j + jstep < V0.na || j == V0.na - 1) ? jstep : V0.na - 1 - j) {
                     double lo = 1e300, hi = -1e300;
-                    for (int v : grp) {
-                        const DevView &V = g.views[v];
+                    for (size_t q = 0; q < grp.size(); ++q) {
+                        const DevView &V = g.views[grp[q]];
                         const double z0 = (V.Sz - g.z_lo) / g.dz;
-                        double emin = 1e300, emax = -1e300;
-                        for (int w = w0; w <= w1; ++w) {
-                            const double e = (g.bz[w] + V.zP - V.Sz) / g.dz;
-                            emin = std::min(emin, e);
-                            emax = std::max(emax, e);
-                        }
+                        const double emin = emins[zb * grp.size() + q], emax = emaxs[zb * grp.size() + q];
                         for (int u : us) {
                             const double ca = V.xdrv ? (g.ux[u] * V.c - g.uy[u] * V.s) : (g.ux[u] * V.s + g.uy[u] * V.c);
                             const double T = (V.a0 - V.Sa + j * g.dx) / (ca - V.Sa);
