@@ -160,7 +160,9 @@ __global__ void __launch_bounds__(kCT, 1) conv3x3_kernel(ConvArgs a)
     unsigned char *s_a = smem + 9 * NCH * CO * 16;      // [3][NCH][kShift] chunks
     __shared__ __align__(8) uint64_t s_bar;
     __shared__ uint32_t s_tmem;
+    __shared__ float s_bias[CO];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid < CO) s_bias[tid] = a.bias ? a.bias[tid] : 0.f;
 
     // the layer's weights, 12 loads in flight per thread
     constexpr int kWChunks = CO * 9 * NCH;
@@ -284,7 +286,7 @@ __global__ void __launch_bounds__(kCT, 1) conv3x3_kernel(ConvArgs a)
         if (ok && y < a.H && x < a.W) {
             const size_t pix = ((size_t)b * a.H + y) * a.W + x;
             if (a.epi == CTLAB_CNN_EPI_RESIDUAL) {
-                a.out_f32[pix] = __uint_as_float(v[0]) + a.bias[0] + a.center[pix];
+                a.out_f32[pix] = __uint_as_float(v[0]) + s_bias[0] + a.center[pix];
             } else {
                 uint4 mk[CO / 8];
                 if (a.epi == CTLAB_CNN_EPI_MASK) {
@@ -298,7 +300,7 @@ __global__ void __launch_bounds__(kCT, 1) conv3x3_kernel(ConvArgs a)
                     for (int e = 0; e < 8; ++e) f[e] = __uint_as_float(v[c8 * 8 + e]);
                     if (a.epi == CTLAB_CNN_EPI_RELU) {
 #pragma unroll
-                        for (int e = 0; e < 8; ++e) f[e] = fmaxf(f[e] + a.bias[c8 * 8 + e], 0.f);
+                        for (int e = 0; e < 8; ++e) f[e] = fmaxf(f[e] + s_bias[c8 * 8 + e], 0.f);
                     } else if (a.epi == CTLAB_CNN_EPI_MASK) {
                         const __nv_bfloat16 *mb = reinterpret_cast<const __nv_bfloat16 *>(&mk[c8]);
 #pragma unroll
