@@ -46,17 +46,17 @@ class OracleViews:
         return out
 
 
-def _scan():
+def _scan(PN):
     import oracle
     from ctlab_b200 import geometry as G
     import ctlab_b200 as cb
-    g = G.small(PN=13)
+    g = G.small(PN=PN)
     hx, hy, hz = G.half_extents(g)
     vol = oracle.ellipsoid_phantom(g, cb.random_ellipsoids(3, hx, hy, hz, 4, 6))
     return g, vol
 
 
-def _rank(rank, world, port):
+def _rank(rank, world, port, PN):
     import torch
     import torch.distributed as dist
 
@@ -67,7 +67,7 @@ def _rank(rank, world, port):
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        g, vol = _scan()
+        g, vol = _scan(PN)
         mask = (np.arange(g.XN * g.YN) % 7 != 0).astype(np.uint8)
         dp = DistributedPlan(OracleViews(g), g.PN)
         prj = torch.zeros(g.prj_shape, dtype=torch.float32)
@@ -89,7 +89,7 @@ def _free_port():
         return s.getsockname()[1]
 
 
-@pytest.mark.parametrize("world", [2, 3])
-def test_distributed_view_split_matches_one_process(world):
+@pytest.mark.parametrize("world,PN", [(2, 13), (3, 13), (2, 12)])  # padded and direct gathers
+def test_distributed_view_split_matches_one_process(world, PN):
     import torch.multiprocessing as mp
-    mp.spawn(_rank, args=(world, _free_port()), nprocs=world, join=True)
+    mp.spawn(_rank, args=(world, _free_port(), PN), nprocs=world, join=True)
