@@ -65,8 +65,9 @@ def parse():
     return ap.parse_args()
 
 
-def workload_geometry(args):
-    from ctlab_b200 import geometry as G
+def workload_geometry(args, G=None):
+    if G is None:
+        from ctlab_b200 import geometry as G
     g = G.config2()
     if args.views:
         runs = max(1, args.views // 8)
@@ -174,39 +175,110 @@ def cpu_sample(g, vol_h, prj_h, nviews):
                       "FP64 oracle with OpenMP, scaled per voxel-view"}
 
 
+def geometry_records():
+    """ctlab_b200/geometry.py loaded on its own (numpy only): the reference arm draws
+    its scan without importing the package or loading the CUDA library."""
+    import importlib.util
+    name = "ctlab_scan_geometry"
+    if name not in sys.modules:
+        spec = importlib.util.spec_from_file_location(name, os.path.join(ROOT, "ctlab_b200", "geometry.py"))
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[name] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules[name]
+
+
 def run_reference(args):
+    """The reference's CPU DD path, restated by the oracle (the reference's own CPU DD
+    bodies are not published), on the host cores with all their threads.  Each timed step
+    projects and backprojects the full 512x512x256 volume over a bounded sample of the
+    984 views (evenly spaced); value = voxel-views processed / measured step time."""
     ws, rank, _ = dist_env()
     if rank != 0:
         return
     import oracle
-    from ctlab_b200 import geometry as G
-    g = G.config2()
+    G = geometry_records()
+    g = workload_geometry(args, G)
     hx, hy, hz = G.half_extents(g)
-    import ctlab_b200 as cb
-    ell = cb.random_ellipsoids(1, hx, hy, hz)
-    small = g.with_views(np.arange(2))
-    vol = oracle.ellipsoid_phantom(g, ell)
-    prj = oracle.dd3_proj(small, vol).astype(np.float32)
-    prj_all = np.zeros(g.prj_shape, np.float32)
-    prj_all[:2] = prj
-    nviews = max(1, args.cpu_views // 2)
+    vol = oracle.ellipsoid_phantom(g, oracle.random_ellipsoids(1, hx, hy, hz))
+    nviews = max(1, args.cpu_views)
+    idx = np.linspace(0, g.PN - 1, nviews).round().astype(int)
+    gs = g.with_views(idx)
+    prj = oracle.dd3_proj(gs, vol).astype(np.float32)  # the sampled views' input to the backprojection
+    threads = oracle.num_threads()
     # untimed warm-up: one short sample (thread pool start-up, page faults)
     if args.warmup > 0:
-        cpu_sample(g, vol, prj_all, 1)
-    vals = []
+        g1 = g.with_views(idx[:1])
+        oracle.dd3_proj(g1, vol)
+        oracle.dd3_back(g1, prj[:1])
+    times = []
     for _ in range(max(1, args.steps)):
-        vals.append(cpu_sample(g, vol, prj_all, nviews)["value"])
-    v = float(np.median(vals))
-    threads = oracle.num_threads()
-    vv2 = 2 * g.voxel_views
+        t0 = time.perf_counter()
+        oracle.dd3_proj(gs, vol)
+        oracle.dd3_back(gs, prj)
+        times.append(time.perf_counter() - t0)
+    t = float(np.median(times))
+    vv2 = 2 * g.XN * g.YN * g.ZN * nviews
+    v = vv2 / t / 1e9
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": vv2 / (v * 1e9) * 1e3, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": config_dict(args), "impl": "reference",
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"each step: {nviews} evenly spaced views of 984, proj + back, FP64 oracle"},
+                             "sample": f"each step: projection + backprojection of the full volume over {nviews} "
+                                       f"evenly spaced views of {g.PN} (median of {len(times)} steps, "
+                                       f"{t:.2f} s each); the full {g.PN}-view step would take "
+                                       f"{t * g.PN / nviews:.0f} s at this rate (extrapolated, not run)"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def kernel_counters(kernel, args):
+    """Per-launch DRAM bytes and warp instructions of `kernel` at this workload from the
+    committed ncu summary (profiles/kernel_counters.json), with the source hash the
+    capture was made from and whether it still matches the kernel's source file."""
+    path = os.path.join(ROOT, "profiles", "kernel_counters.json")
+    if not os.path.exists(path) or args.views or args.sat != "zprefix":
+        return None
+    entry = json.load(open(path)).get(kernel)
+    if not entry:
+        return None
+    import hashlib
+    src = os.path.join(ROOT, "ctlab_b200", "csrc", entry["source"])
+    cur = hashlib.sha256(open(src, "rb").read()).hexdigest()[:16] if os.path.exists(src) else None
+    return dict(entry, source_matches=(cur == entry.get("source_sha16")))
+
+
+def roofline_entry(dom, t_dom, alg, achieved, peak, peak_kind, clocks, args):
+    """Three views of the dominant kernel against its limits:
+    nominal_frac -- model bytes (8 B per voxel-view + 4 B per detector bin, a
+        view-at-a-time stream of the FP64 SAT / accumulator) / time / HBM peak; this
+        model is not a lower bound on traffic, so kernels that keep data on chip
+        across views and slices exceed 1.0 here;
+    dram_frac -- DRAM bytes one launch actually moves (ncu dram__bytes_read.sum +
+        dram__bytes_write.sum, one full-size launch) / time / HBM peak;
+    issue_frac -- warp instructions one launch executes (ncu smsp__inst_executed.sum)
+        / (148 SMs x 4 schedulers x the median SM clock sampled during the timed region
+        x time): the instruction-issue roofline of these gather kernels."""
+    r = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+         "frac": achieved / peak, "nominal_frac": achieved / peak,
+         "peak_source": ("measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                         else "fallback (6.65 TB/s, earlier measurement on this pool; no MEASURED_PEAKS.json)"),
+         "algorithmic_bytes_per_launch": alg, "launch_ms": t_dom,
+         "traffic": None, "dram_frac": None, "issue_frac": None}
+    c = kernel_counters(dom, args)
+    if c:
+        t = t_dom * 1e-3
+        r["traffic"] = c["dram_bytes_per_launch"]
+        r["dram_achieved_gbs"] = c["dram_bytes_per_launch"] / t / 1e9
+        r["dram_frac"] = r["dram_achieved_gbs"] / peak
+        mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
+        issue_peak = 148 * 4 * mhz * 1e6  # warp instructions per second
+        r["warp_inst_per_launch"] = c["warp_inst_per_launch"]
+        r["issue_frac"] = c["warp_inst_per_launch"] / t / issue_peak
+        r["counters_source"] = (f"profiles/kernel_counters.json ({c['profile']}, captured {c['captured']}; "
+                                f"kernel source {'unchanged' if c['source_matches'] else 'CHANGED'} since)")
+    return r
 
 
 def run_ours(args):
@@ -296,10 +368,6 @@ def run_ours(args):
         dom = "dd3_back_t_kernel" if zp else "dd3_back_kernel"
     t_dom = max(t_proj, t_back)
     achieved = alg / (t_dom * 1e-3) / 1e9
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "dram_bytes.json")
-    if os.path.exists(tp):
-        traffic = json.load(open(tp)).get(dom)
 
     # e2e through the host entry points with pinned buffers
     e2e = None
@@ -338,22 +406,19 @@ def run_ours(args):
         cpu = cpu_sample(g, vol.cpu().numpy(), prj_in.cpu().numpy(), args.cpu_views)
 
     if rank == 0:
+        clocks = clk.summary()
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": {"fp64": "f32 (f64 SAT)", "f32pair": "f32 (f32-pair SAT)",
                                             "zprefix": "f32 (f64-accumulated z-prefix SAT)"}[args.sat],
             "data": "synthetic (seeded random-ellipsoid phantoms)",
-            "config": config_dict(args, {"parallelism": f"independent volume per GPU x{ws}"}),
-            "clocks": clk.summary(),
+            "config": config_dict(args),
+            "parallelism": f"independent volume per GPU x{ws}",
+            "clocks": clocks,
             "e2e": e2e,
             "gpu_launches": launches_per_step * args.steps,
-            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak,
-                         "peak_source": ("measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
-                                         else "fallback (6.65 TB/s, earlier measurement on this pool; no MEASURED_PEAKS.json)"),
-                         "traffic": traffic, "algorithmic_bytes_per_launch": alg,
-                         "launch_ms": t_dom},
+            "roofline": roofline_entry(dom, t_dom, alg, achieved, peak, peak_kind, clocks, args),
             "kernels_ms": {"proj_sat": float(np.mean(proj_sat)), "proj": t_proj,
                            "back_sat": float(np.mean(back_sat)), "back": t_back},
             "proj_gvvps": vv / (t_proj + float(np.mean(proj_sat))) / 1e6,

@@ -117,6 +117,8 @@ _SIGNATURES = {
                                           C.POINTER(C.c_double), C.c_int, C.c_int, _vp]),
     "ctlab_debug_scan_stall": (C.c_int, [C.c_int, C.c_uint]),
     "ctlab_volume_sat_noalloc": (C.c_int, [_vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp, C.c_int, _vp]),
+    "ctlab_noalloc_check": (C.c_int, [_vp]),
+    "ctlab_debug_noalloc_stall": (C.c_int, [C.c_uint, _vp]),
     "ctlab_random_ellipsoids": (C.c_int, [C.c_ulonglong, C.c_int, C.c_int, C.c_float, C.c_float,
                                           C.c_float, C.c_float, C.POINTER(C.c_double), C.c_int]),
 }

@@ -266,8 +266,7 @@ __global__ void __launch_bounds__(kCT, 1) conv3x3_kernel(ConvArgs a)
         }
         // the next tile's halo loads are in flight while the MMAs run
         load_halo(tile + gridDim.x);
-        if (!mbar_wait(&s_bar, phase)) ok = false;
-        phase ^= 1u;
+        const bool waited = mbar_wait(&s_bar, phase);
         __syncwarp();
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 
@@ -283,7 +282,7 @@ __global__ void __launch_bounds__(kCT, 1) conv3x3_kernel(ConvArgs a)
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         const int m = warp * 32 + lane;
         const int y = y0 + m / kTW, x = x0 + m % kTW;
-        if (ok && y < a.H && x < a.W) {
+        if (waited && y < a.H && x < a.W) {
             const size_t pix = ((size_t)b * a.H + y) * a.W + x;
             if (a.epi == CTLAB_CNN_EPI_RESIDUAL) {
                 a.out_f32[pix] = __uint_as_float(v[0]) + s_bias[0] + a.center[pix];
@@ -315,11 +314,21 @@ __global__ void __launch_bounds__(kCT, 1) conv3x3_kernel(ConvArgs a)
                 }
             }
         }
-        // TMEM and the shifted tiles are free for the next tile
+        // TMEM and the shifted tiles are free for the next tile -- unless any
+        // thread's wait ran out: then the whole CTA stops (no further halo
+        // stores or MMAs) after one more bounded wait for the MMAs in flight,
+        // so that tensor memory is not freed under them.  The launch's output
+        // is invalid once g_cnn_err is set.
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
+        if (__syncthreads_or(!waited)) {
+            if (tid == 0) (void)mbar_wait(&s_bar, phase);
+            __syncthreads();
+            ok = false;
+            break;
+        }
+        phase ^= 1u;
     }
-    if (!ok) atomicExch(&g_cnn_err, 1);
+    if (!ok && tid == 0) atomicExch(&g_cnn_err, 1);
     __syncwarp();
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");

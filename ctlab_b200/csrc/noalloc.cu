@@ -90,9 +90,63 @@ extern "C" int ctlab_volume_sat_noalloc(const float *d_vol, const unsigned char 
     st.agg = reinterpret_cast<double *>(base + kHeader + flag_bytes);
     st.pref = reinterpret_cast<double *>(base + kHeader + flag_bytes + vec_bytes);
     cudaStream_t s = (cudaStream_t)stream;
-    // The array keeps the previous call's contents: the error word is
-    // cleared here, the ticket and the flags by the scan launch itself.
-    CTLAB_CUDA_TRY(cudaMemsetAsync(st.err, 0, sizeof(int), s));
+    // The array keeps the previous call's contents.  The scan launch zeroes
+    // the ticket and the flags itself; the error word is left alone so that
+    // a timeout stays visible until ctlab_noalloc_check reads and clears it.
     CTLAB_CUDA_TRY(launch_volume_sat(d_vol, d_mask, XN, YN, ZN, orientation, d_sat, zp, 0, st, kChunk, s));
+    return ok();
+}
+
+extern "C" int ctlab_noalloc_check(void *stream)
+{
+    using namespace ctlab;
+    int dev = 0;
+    CTLAB_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return set_status(CTLAB_ERR_INVALID_ARG, "device index beyond 64");
+    unsigned char *base = nullptr;
+    int rc = scratch_address(dev, &base);
+    if (rc != CTLAB_OK) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    int *err = reinterpret_cast<int *>(base + sizeof(int));
+    int h_err = 0;
+    CTLAB_CUDA_TRY(cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CTLAB_CUDA_TRY(cudaStreamSynchronize(s));
+    if (h_err != 0) {
+        CTLAB_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int), s));
+        CTLAB_CUDA_TRY(cudaStreamSynchronize(s));
+        return set_status(CTLAB_ERR_TIMEOUT,
+                          "a bounded wait in an allocation-free SAT scan timed out; its output is invalid");
+    }
+    return ok();
+}
+
+// Diagnostics for ctlab_noalloc_check: the lookback scan of a 2-row plane
+// whose first chunk never publishes, with all of its state (and its tiny
+// input and output) inside the fixed array.  The second chunk's bounded wait
+// runs out after spin_limit polls and raises the array's error word.
+extern "C" int ctlab_debug_noalloc_stall(unsigned spin_limit, void *stream)
+{
+    using namespace ctlab;
+    if (spin_limit < 1 || spin_limit > (1u << 24))
+        return set_status(CTLAB_ERR_INVALID_ARG, "spin_limit must be in [1, 2^24]");
+    int dev = 0;
+    CTLAB_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return set_status(CTLAB_ERR_INVALID_ARG, "device index beyond 64");
+    unsigned char *base = nullptr;
+    int rc = scratch_address(dev, &base);
+    if (rc != CTLAB_OK) return rc;
+    constexpr int rows = 2, nk = 8;
+    // header | flags @256 | agg @512 | pref @768 | input @1024 | output @1280 (ends at 1496)
+    ScanState st;
+    st.ticket = reinterpret_cast<int *>(base);
+    st.err = reinterpret_cast<int *>(base + sizeof(int));
+    st.flags = reinterpret_cast<int *>(base + kHeader);
+    st.agg = reinterpret_cast<double *>(base + 512);
+    st.pref = reinterpret_cast<double *>(base + 768);
+    float *vol = reinterpret_cast<float *>(base + 1024);
+    double *out = reinterpret_cast<double *>(base + 1280);
+    cudaStream_t s = (cudaStream_t)stream;
+    CTLAB_CUDA_TRY(cudaMemsetAsync(vol, 0, sizeof(float) * rows * nk, s));
+    CTLAB_CUDA_TRY(launch_scan_stall(vol, rows, nk, out, st, 1, spin_limit, s));
     return ok();
 }

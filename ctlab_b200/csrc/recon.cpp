@@ -225,6 +225,9 @@ int ctlab_os_sart(ctlab_plan *plan, float *d_x, const float *d_meas, const unsig
             if (rc == CTLAB_OK)
                 rc = plan_back_list(plan, lst, n, d_mask, d_cols + nv * k, s, BACK_PLAIN, nullptr, 1.f, 0, 0.f, 0.f);
         }
+        // a scan that timed out while the weights were built leaves them
+        // invalid: they are kept only once the device error word is clear
+        if (rc == CTLAB_OK) rc = plan_check_device_error(plan, s);
         if (rc != CTLAB_OK) return rc;
         W.key = key;
         W.weights = true;

@@ -156,9 +156,24 @@ int ctlab_volume_sat(ctlab_plan *plan, const float *d_vol, const unsigned char *
  * a device looks up the array's device address; make that call before any
  * stream capture.  All calls share the array, so calls that overlap on the
  * GPU (other streams, other threads) race; serialise them.  Asynchronous on
- * `stream`.  No counterpart in the reference. */
+ * `stream`: a lookback wait that runs out inside the scan cannot be
+ * returned here; it raises the array's error word, which
+ * ctlab_noalloc_check reports.  No counterpart in the reference. */
 int ctlab_volume_sat_noalloc(const float *d_vol, const unsigned char *d_mask, int XN, int YN, int ZN,
                              int orientation, double *d_sat, int zp, void *stream);
+
+/* Waits for `stream` and reports whether any allocation-free call on the
+ * current device since the previous check hit a bounded-wait timeout:
+ * CTLAB_ERR_TIMEOUT (the output of that call is invalid) or CTLAB_OK.  The
+ * error word is sticky until this call reads it and clears it.  Allocates
+ * nothing.  No counterpart in the reference. */
+int ctlab_noalloc_check(void *stream);
+
+/* Diagnostics: runs a two-chunk lookback scan on the allocation-free array
+ * whose first chunk never publishes, so that the second chunk's bounded
+ * wait (spin_limit polls, 1..2^24) runs out and raises the error word that
+ * ctlab_noalloc_check reports.  No counterpart in the reference. */
+int ctlab_debug_noalloc_stall(unsigned spin_limit, void *stream);
 
 /* Copies the plan's volume SAT of one orientation to d_out (FP64 plans:
  * doubles, [planes][rows][zp] as reported by ctlab_plan_sat_layout;

@@ -65,6 +65,11 @@ def load() -> C.CDLL:
                                                 C.c_double, _u8, C.c_int, C.c_float, C.c_double, C.c_float,
                                                 C.c_float]
         lib.orc_fista_tv.restype = C.c_int
+        lib.orc_view_frame.argtypes = [C.c_double, C.c_double, C.c_double, C.c_float, C.c_float, _dp]
+        lib.orc_view_to_world.argtypes = [C.c_float, C.c_float, _dp, _dp]
+        lib.orc_random_ellipsoids.argtypes = [C.c_ulonglong, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float,
+                                              C.c_float, _dp, C.c_int]
+        lib.orc_random_ellipsoids.restype = C.c_int
         lib.orc_num_threads.restype = C.c_int
         lib.orc_set_num_threads.argtypes = [C.c_int]
         _lib = lib
@@ -144,6 +149,17 @@ def ellipsoid_phantom(g, ell, clamp_nonneg=True) -> np.ndarray:
                                  e.ctypes.data_as(_dp), e.shape[0], 1 if clamp_nonneg else 0,
                                  out.ctypes.data_as(_fp))
     return out
+
+
+def random_ellipsoids(seed: int, half_x: float, half_y: float, half_z: float, n_min: int = 20, n_max: int = 40,
+                      v_max: float = 0.03) -> np.ndarray:
+    """The seeded random-ellipsoid records of the synthetic workloads (phantom_rng.cpp)."""
+    buf = np.zeros((n_max, 10), np.float64)
+    n = load().orc_random_ellipsoids(seed, n_min, n_max, half_x, half_y, half_z, v_max, buf.ctypes.data_as(_dp),
+                                     n_max)
+    if n < 0:
+        raise ValueError("bad random-ellipsoid arguments")
+    return buf[:n].copy()
 
 
 def ellipsoid_line_integral(ell, p0, p1) -> float:

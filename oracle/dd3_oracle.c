@@ -149,6 +149,27 @@ static orc_view make_view(double x0, double y0, double z0, float ang, float zP)
     return v;
 }
 
+/* A view's frame as make_view builds it: out = {cos, sin, zP, Sx, Sy, Sz,
+ * x-driven}.  Exported so the tests can pin the oracle's rotation. */
+void orc_view_frame(double x0, double y0, double z0, float ang, float zP, double *out)
+{
+    orc_view v = make_view(x0, y0, z0, ang, zP);
+    out[0] = v.c; out[1] = v.s; out[2] = v.zP;
+    out[3] = v.Sx; out[4] = v.Sy; out[5] = v.Sz;
+    out[6] = (double)v.xdrv;
+}
+
+/* View-local point -> world with the rotation make_view uses (world =
+ * R(theta) local + (0, 0, zP)); the inverse of the reference's invRotVox,
+ * src/utilities.cuh:289-298, which the tests check it against. */
+void orc_view_to_world(float ang, float zP, const double *local3, double *world3)
+{
+    orc_view v = make_view(0.0, 0.0, 0.0, ang, zP);
+    world3[0] = local3[0] * v.c - local3[1] * v.s;
+    world3[1] = local3[0] * v.s + local3[1] * v.c;
+    world3[2] = local3[2] + v.zP;
+}
+
 static void boundaries_f(int n, const float *cf, double *b)
 {
     if (n < 1) return;

@@ -107,3 +107,14 @@ def test_row_and_column_sums_positive_inside_fov():
     cols = oracle.dd3_back(g, np.ones(g.prj_shape, np.float32))
     assert rows.max() > 0 and np.all(rows >= 0)
     assert np.all(cols > 0)
+
+
+def test_config2_switch_views_sit_on_both_sides_of_each_hand_over():
+    """The hand-over views of the config-2 parity case (GPU test) straddle every
+    x/y-driven switch angle after float32 rounding: just below, on, just above pi/4,
+    3pi/4, 5pi/4, 7pi/4 (float32(5pi/4) and float32(7pi/4) round below the angle)."""
+    from test_gpu_parity_configs import config2_switch_geometry
+    lib = oracle.load()
+    g = config2_switch_geometry()
+    xd = [lib.orc_view_is_xdriven(lib.orc_regularize_angle(float(a))) for a in g.hangs]
+    assert xd[24:] == [0, 1, 1, 1, 0, 0, 0, 0, 1, 1, 1, 0]

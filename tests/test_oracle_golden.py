@@ -31,12 +31,36 @@ def test_regularize_angle_matches_reference():
     assert np.all((got >= 0) & (got < 2 * np.pi))
 
 
-def test_rotation_convention_matches_inv_rot_vox():
-    # invRotVox maps world -> rotated frame: x' = x c + y s, y' = -x s + y c, z' = z - zP
-    v, th, zp = GOLD["rot_in"], GOLD["rot_th"], GOLD["rot_zp"]
-    c, s = np.cos(th).astype(np.float32), np.sin(th).astype(np.float32)
-    exp = np.stack([v[:, 0] * c + v[:, 1] * s, -v[:, 0] * s + v[:, 1] * c, v[:, 2] - zp], 1)
-    np.testing.assert_allclose(exp, GOLD["rot_out"], rtol=1e-5, atol=1e-4)
+def test_oracle_rotation_inverts_inv_rot_vox():
+    """The oracle's own view rotation (make_view, through orc_view_to_world) undoes the
+    reference's compiled invRotVox (world -> view frame): mapping invRotVox's outputs
+    back to the world returns its inputs."""
+    lib = oracle.load()
+    v, th, zp, rot = GOLD["rot_in"], GOLD["rot_th"], GOLD["rot_zp"], GOLD["rot_out"]
+    for i in range(v.shape[0]):
+        loc = np.ascontiguousarray(rot[i], np.float64)
+        out = np.zeros(3)
+        lib.orc_view_to_world(np.float32(th[i]), zp[i], loc.ctypes.data_as(C.POINTER(C.c_double)),
+                              out.ctypes.data_as(C.POINTER(C.c_double)))
+        np.testing.assert_allclose(out, v[i], rtol=1e-5, atol=2e-4)
+
+
+def test_oracle_view_frame_places_the_source_by_the_same_rotation():
+    """make_view's source position is the view-to-world image of (x0, y0, z0), its
+    driving axis follows the quadrant constants, and the angle is regularised first."""
+    lib = oracle.load()
+    dp = C.POINTER(C.c_double)
+    x0, y0, z0 = 3.0, 541.0, -2.0
+    for ang in (0.0, 0.3, np.pi / 4, 2.0, 3.9, 5.5, -1.0, 7.0):
+        fr = np.zeros(7)
+        lib.orc_view_frame(x0, y0, z0, np.float32(ang), np.float32(1.5), fr.ctypes.data_as(dp))
+        w = np.zeros(3)
+        lib.orc_view_to_world(np.float32(ang), np.float32(1.5), np.array([x0, y0, z0]).ctypes.data_as(dp),
+                              w.ctypes.data_as(dp))
+        np.testing.assert_allclose(fr[3:6], w, rtol=0, atol=1e-9)
+        th = lib.orc_regularize_angle(float(np.float32(ang)))
+        assert fr[6] == lib.orc_view_is_xdriven(th)
+        np.testing.assert_allclose(fr[:2], [np.cos(th), np.sin(th)], atol=1e-15)
 
 
 def test_sart_weightings_match_reference():

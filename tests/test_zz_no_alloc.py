@@ -55,6 +55,34 @@ def test_noalloc_volume_sat_matches_plan_path_on_two_calls(torch_cuda):
             b = ref.view(planes, rows, zp)[:, :, : g.ZN + 1].cpu().numpy()
             assert np.all(np.isfinite(a)), f"call {call} orientation {o}: unwritten entries"
             np.testing.assert_allclose(a, b, rtol=TOL, atol=TOL * np.abs(b).max())
+    assert lib.ctlab_noalloc_check(stream) == cb.CTLAB_OK, lib.ctlab_last_error()
+
+
+def test_noalloc_check_reports_a_timed_out_scan_once(torch_cuda):
+    """A scan on the fixed array whose lookback wait runs out (its first chunk never
+    publishes) is reported by ctlab_noalloc_check as a timeout, once; the error word is
+    then clear, and the next allocation-free SAT is valid and checks clean."""
+    torch = torch_cuda
+    lib = cb.load()
+    stream = torch.cuda.current_stream().cuda_stream
+    assert lib.ctlab_noalloc_check(stream) == cb.CTLAB_OK, lib.ctlab_last_error()
+    assert lib.ctlab_debug_noalloc_stall(2000, stream) == cb.CTLAB_OK, lib.ctlab_last_error()
+    rc = lib.ctlab_noalloc_check(stream)
+    assert rc == cb.CTLAB_ERR_TIMEOUT, lib.ctlab_last_error()
+    assert b"timed out" in lib.ctlab_last_error()
+    assert lib.ctlab_noalloc_check(stream) == cb.CTLAB_OK  # read and cleared
+    # the context and the array stay usable
+    g = G.small(PN=4, XN=20, YN=18, ZN=9, start=0.0)
+    vol = torch.rand(g.vol_shape, dtype=torch.float32, device="cuda")
+    zp = g.ZN + 1
+    out = torch.zeros(g.YN * (g.XN + 1) * zp, dtype=torch.float64, device="cuda")
+    assert lib.ctlab_volume_sat_noalloc(vol.data_ptr(), None, g.XN, g.YN, g.ZN, 0, out.data_ptr(), zp,
+                                        stream) == cb.CTLAB_OK
+    assert lib.ctlab_noalloc_check(stream) == cb.CTLAB_OK, lib.ctlab_last_error()
+    v = vol.double().cpu().numpy()  # [y][x][z]
+    ref = np.zeros((g.YN, g.XN + 1, zp))
+    ref[:, 1:, 1:] = np.cumsum(np.cumsum(v, axis=1), axis=2)
+    np.testing.assert_allclose(out.view(g.YN, g.XN + 1, zp).cpu().numpy(), ref, rtol=TOL, atol=1e-10)
 
 
 def test_noalloc_volume_sat_rejects_volumes_beyond_its_scratch(torch_cuda):
