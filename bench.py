@@ -11,9 +11,11 @@ included.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-With N > 1 (torchrun), every rank projects and backprojects its own
-independent random-ellipsoid volume (weak scaling, no data-path collective);
-timing is the max over ranks.  --impl reference times the CPU restatement of
+With N > 1 (torchrun), the ranks share one scan (--split scan, the default):
+projection split by views, backprojection by z slabs, NCCL all-gathers of the
+view blocks and slabs (strong scaling); --split volumes gives every rank its
+own independent volume instead (weak scaling, no data-path collective).
+Timing is the max over ranks.  --impl reference times the CPU restatement of
 the reference's DD path (the oracle) on the host cores instead.
 """
 from __future__ import annotations
@@ -59,6 +61,11 @@ def parse():
     ap.add_argument("--recon-iters", type=int, default=0,
                     help="recon workload: iterations of each solver (0 = 30 OS-SART, 50 FISTA-TV); a smaller count "
                          "is a profiling case")
+    ap.add_argument("--split", default="auto", choices=["auto", "scan", "volumes"],
+                    help="'scan' splits one scan over the ranks (projection by views, backprojection by z slabs, "
+                         "NCCL all-gathers of the view blocks and slabs; strong scaling); 'volumes' gives every "
+                         "rank its own independent volume (weak scaling, no data-path collective); 'auto' = scan "
+                         "for N > 1, the plain one-GPU path for N = 1")
     ap.add_argument("--views", type=int, default=0,
                     help="profiling case: keep only this many of the 984 views, in evenly spaced runs of 8 "
                          "adjacent views (0 = all)")
@@ -281,6 +288,122 @@ def roofline_entry(dom, t_dom, alg, achieved, peak, peak_kind, clocks, args):
     return r
 
 
+def run_split(args):
+    """N ranks share ONE scan: rank r projects its block of the 984 views of the whole
+    (replicated) volume and backprojects its z slab of the volume from the views that
+    reach it; the view blocks and the slabs are all-gathered over NCCL, so every rank
+    ends the step holding the whole projection and the whole backprojection.  value =
+    the scan's voxel-views (2 * XN*YN*ZN*PN per step) / the max-over-ranks step time.
+    e2e: the same step with the volume and the input projection uploaded from pinned
+    host memory on every rank and both results read back, inside the timed region."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    import ctlab_b200 as cb
+    from ctlab_b200 import geometry as G
+    from ctlab_b200.multi import DistributedPlan
+
+    ws, rank, local = dist_env()
+    if "MASTER_ADDR" not in os.environ:  # a one-rank group outside torchrun
+        import socket
+        with socket.socket() as so:
+            so.bind(("127.0.0.1", 0))
+            os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(so.getsockname()[1]))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", init_method="env://", world_size=ws, rank=rank,
+                            timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    g = workload_geometry(args)
+    hx, hy, hz = G.half_extents(g)
+    sat_mode = {"fp64": cb.CTLAB_SAT_FP64, "f32pair": cb.CTLAB_SAT_F32PAIR, "zprefix": cb.CTLAB_SAT_ZPREFIX}[args.sat]
+    plans = []
+
+    def make_plan(geom):
+        plans.append(cb.Plan(geom, device=local, sat_mode=sat_mode))
+        return plans[-1]
+
+    dp = DistributedPlan(g, make_plan)
+    vol = torch.zeros(g.vol_shape, dtype=torch.float32, device="cuda")
+    cb.ellipsoid_phantom(vol, g, cb.random_ellipsoids(1, hx, hy, hz))  # the same scan on every rank
+    prj_in = torch.zeros(g.prj_shape, dtype=torch.float32, device="cuda")
+    dp.proj(vol, prj_in)
+    prj = torch.zeros_like(prj_in)
+    back = torch.zeros_like(vol)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        dp.proj(vol, prj)
+        dp.back(prj_in, back)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    step()
+    launches_per_step = sum(p.last_launches() for p in plans)
+    torch.cuda.synchronize()
+
+    def timed(fn, steps):
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        dist.barrier()
+        t = torch.tensor([e0.elapsed_time(e1) / steps], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    with ClockSampler(local) as clk:
+        ms_step = timed(step, args.steps)
+    vv = g.voxel_views
+    value = 2 * vv / (ms_step * 1e-3) / 1e9
+
+    e2e = None
+    if not args.no_e2e:
+        hvol = torch.empty(g.vol_shape, dtype=torch.float32, pin_memory=True)
+        hvol.copy_(vol.cpu())
+        hprj_in = torch.empty(g.prj_shape, dtype=torch.float32, pin_memory=True)
+        hprj_in.copy_(prj_in.cpu())
+        hprj = torch.empty(g.prj_shape, dtype=torch.float32, pin_memory=True)
+        hback = torch.empty(g.vol_shape, dtype=torch.float32, pin_memory=True)
+        dvol, dprj_in = torch.empty_like(vol), torch.empty_like(prj_in)
+
+        def e2e_step():
+            dvol.copy_(hvol, non_blocking=True)
+            dprj_in.copy_(hprj_in, non_blocking=True)
+            dp.proj(dvol, prj)
+            dp.back(dprj_in, back)
+            hprj.copy_(prj, non_blocking=True)
+            hback.copy_(back, non_blocking=True)
+
+        for _ in range(2):
+            e2e_step()
+        es = timed(e2e_step, args.steps)
+        nb = 4 * (g.XN * g.YN * g.ZN + g.PN * g.DNU * g.DNV) * ws
+        e2e = {"value": 2 * vv / (es * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": nb,
+               "d2h_bytes_per_step": nb, "ms_per_step": es,
+               "path": "DistributedPlan.proj + .back (pinned host buffers on every rank)"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": max(3, args.warmup), "ms_per_step": ms_step, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None,
+                "dtype": {"fp64": "f32 (f64 SAT)", "f32pair": "f32 (f32-pair SAT)",
+                          "zprefix": "f32 (f64-accumulated z-prefix SAT)"}[args.sat],
+                "data": "synthetic (seeded random-ellipsoid phantom)", "config": config_dict(args),
+                "parallelism": f"one scan over {ws} ranks: views (projection) and z slabs (backprojection), "
+                               "NCCL all-gather of view blocks and slabs",
+                "clocks": clk.summary(), "e2e": e2e, "gpu_launches": launches_per_step * args.steps * ws,
+                "roofline": None, "cpu_baseline": None}
+        print(json.dumps(line), flush=True)
+    dp.close()
+    dist.barrier()
+    dist.destroy_process_group()
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -289,6 +412,8 @@ def run_ours(args):
     from ctlab_b200 import geometry as G
 
     ws, rank, local = dist_env()
+    if args.split == "scan" or (ws > 1 and args.split == "auto"):
+        return run_split(args)
     torch.cuda.set_device(local)
     if ws > 1:
         dist.init_process_group("nccl", init_method="env://", world_size=ws, rank=rank,
@@ -369,37 +494,47 @@ def run_ours(args):
     t_dom = max(t_proj, t_back)
     achieved = alg / (t_dom * 1e-3) / 1e9
 
-    # e2e through the host entry points with pinned buffers
+    # e2e through the host entry points: pinned host buffers (the headline), and
+    # pageable ones (numpy arrays, what thrust::host_vector callers pass) beside it
     e2e = None
     if not args.no_e2e:
+        gargs = g.args()
+
+        def e2e_time(hv, hp, hb):
+            def e2e_step():
+                cb.DD3Proj_gpu(**gargs, hvol=hv, hprj=hp, mask=None, gpunum=local, prjMode=0)
+                cb.DD3Back_gpu(**gargs, hvol=hb, hprj=hp, mask=None, gpunum=local, squared=0, prjMode=0)
+
+            for _ in range(max(2, args.warmup)):
+                e2e_step()
+            barrier()
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                e2e_step()
+            t1 = time.perf_counter()
+            barrier()
+            es = (t1 - t0) / args.steps
+            if ws > 1:
+                t = torch.tensor([es], device="cuda", dtype=torch.float64)
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                es = float(t.item())
+            return es
+
         hvol = torch.empty(g.vol_shape, dtype=torch.float32, pin_memory=True)
         hvol.copy_(vol.cpu())
         hprj = torch.empty(g.prj_shape, dtype=torch.float32, pin_memory=True)
         hback = torch.empty(g.vol_shape, dtype=torch.float32, pin_memory=True)
-        hv, hp, hb = hvol.numpy(), hprj.numpy(), hback.numpy()
-        gargs = g.args()
-
-        def e2e_step():
-            cb.DD3Proj_gpu(**gargs, hvol=hv, hprj=hp, mask=None, gpunum=local, prjMode=0)
-            cb.DD3Back_gpu(**gargs, hvol=hb, hprj=hp, mask=None, gpunum=local, squared=0, prjMode=0)
-
-        for _ in range(max(2, args.warmup)):
-            e2e_step()
-        barrier()
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            e2e_step()
-        t1 = time.perf_counter()
-        barrier()
-        es = (t1 - t0) / args.steps
-        if ws > 1:
-            t = torch.tensor([es], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            es = float(t.item())
+        es = e2e_time(hvol.numpy(), hprj.numpy(), hback.numpy())
+        pv = hvol.numpy().copy()  # pageable copies, first-touched before timing
+        pp, pb = np.zeros(g.prj_shape, np.float32), np.zeros(g.vol_shape, np.float32)
+        es_pg = e2e_time(pv, pp, pb)
+        del hvol, hprj, hback
         nvb, npb = 4 * vv // g.PN, 4 * g.PN * g.DNU * g.DNV
         e2e = {"value": ws * 2 * vv / es / 1e9, "unit": UNIT, "h2d_bytes_per_step": nvb + npb,
                "d2h_bytes_per_step": npb + nvb, "ms_per_step": es * 1e3,
-               "path": "DD3Proj_gpu + DD3Back_gpu (host pointers, pinned)"}
+               "path": "DD3Proj_gpu + DD3Back_gpu (host pointers, pinned)",
+               "pageable": {"value": ws * 2 * vv / es_pg / 1e9, "ms_per_step": es_pg * 1e3,
+                            "path": "DD3Proj_gpu + DD3Back_gpu (host pointers, pageable numpy arrays)"}}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:

@@ -71,6 +71,15 @@ _SIGNATURES = {
     "DD3Back_gpu": (None, [C.c_float, C.c_float, C.c_float, C.c_int, C.c_int, _fp, _fp, _fp,
                            C.c_float, C.c_float, C.c_float, _fp, _fp, C.c_int, C.c_int, C.c_int,
                            C.c_int, _fp, _fp, C.c_float, C.c_float, _u8p, C.c_int, C.c_int, C.c_int]),
+    "DD3Proj_multiGPU": (None, [C.c_float, C.c_float, C.c_float, C.c_int, C.c_int, _fp, _fp, _fp,
+                                C.c_float, C.c_float, C.c_float, _fp, _fp, C.c_int, C.c_int, C.c_int,
+                                C.c_int, _fp, _fp, C.c_float, C.c_float, _u8p, C.c_int, _ip, C.c_int]),
+    "DD3Back_multiGPU": (None, [C.c_float, C.c_float, C.c_float, C.c_int, C.c_int, _fp, _fp, _fp,
+                                C.c_float, C.c_float, C.c_float, _fp, _fp, C.c_int, C.c_int, C.c_int,
+                                C.c_int, _fp, _fp, C.c_float, C.c_float, _u8p, C.c_int, _ip, C.c_int]),
+    "ctlab_slab_views": (C.c_int, [C.POINTER(Geometry), C.c_int, C.c_int, _ip, C.c_int]),
+    "ctlab_proj_multi": (C.c_int, [C.POINTER(Geometry), _vp, _vp, _vp, _ip, C.c_int]),
+    "ctlab_back_multi": (C.c_int, [C.POINTER(Geometry), _vp, _vp, _vp, _ip, C.c_int]),
     "ctlab_last_status": (C.c_int, []),
     "ctlab_last_error": (C.c_char_p, []),
     "ctlab_plan_create": (C.c_int, [C.POINTER(Geometry), C.c_int, C.c_int, C.POINTER(_vp)]),

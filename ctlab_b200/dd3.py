@@ -62,6 +62,80 @@ def DD3Back_gpu(x0, y0, z0, DNU, DNV, xds, yds, zds, imgXCenter, imgYCenter, img
     check_last()
 
 
+def DD3Proj_multiGPU(x0, y0, z0, DNU, DNV, xds, yds, zds, imgXCenter, imgYCenter, imgZCenter, hangs, hzPos,
+                     PN, XN, YN, ZN, hvol, hprj, dx, dz, mask, prjMode, startPN, gpuNum):
+    """One scan's views split over ``gpuNum`` GPUs: GPU i projects views
+    [startPN[i], startPN[i+1]).  Same arguments as the reference's DD3Proj_multiGPU."""
+    lib = load()
+    xds, yds, zds, hangs, hzPos = map(_f32, (xds, yds, zds, hangs, hzPos))
+    _require(hvol, np.float32, XN * YN * ZN, "hvol")
+    _require(hprj, np.float32, PN * DNU * DNV, "hprj")
+    m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+    if m is not None and m.size != XN * YN:
+        raise CtlabError(_lib.CTLAB_ERR_INVALID_ARG, "mask must hold XN*YN bytes")
+    st = np.ascontiguousarray(startPN, dtype=np.int32)
+    if st.size < gpuNum:
+        raise CtlabError(_lib.CTLAB_ERR_INVALID_ARG, "startPN must hold gpuNum entries")
+    lib.DD3Proj_multiGPU(x0, y0, z0, DNU, DNV, _ptr(xds), _ptr(yds), _ptr(zds), imgXCenter, imgYCenter,
+                         imgZCenter, _ptr(hangs), _ptr(hzPos), PN, XN, YN, ZN, _ptr(hvol), _ptr(hprj), dx, dz,
+                         None if m is None else m.ctypes.data, prjMode, st.ctypes.data_as(C.POINTER(C.c_int)),
+                         gpuNum)
+    check_last()
+
+
+def DD3Back_multiGPU(x0, y0, z0, DNU, DNV, xds, yds, zds, imgXCenter, imgYCenter, imgZCenter, hangs, hzPos,
+                     PN, XN, YN, ZN, hvol, hprj, dx, dz, mask, methodId, startVOL, gpuNum):
+    """One scan's volume split into z slabs over ``gpuNum`` GPUs: GPU i backprojects
+    slices [startVOL[i], startVOL[i+1]).  Same arguments as DD3Back_multiGPU."""
+    lib = load()
+    xds, yds, zds, hangs, hzPos = map(_f32, (xds, yds, zds, hangs, hzPos))
+    _require(hvol, np.float32, XN * YN * ZN, "hvol")
+    _require(hprj, np.float32, PN * DNU * DNV, "hprj")
+    m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+    if m is not None and m.size != XN * YN:
+        raise CtlabError(_lib.CTLAB_ERR_INVALID_ARG, "mask must hold XN*YN bytes")
+    st = np.ascontiguousarray(startVOL, dtype=np.int32)
+    if st.size < gpuNum:
+        raise CtlabError(_lib.CTLAB_ERR_INVALID_ARG, "startVOL must hold gpuNum entries")
+    lib.DD3Back_multiGPU(x0, y0, z0, DNU, DNV, _ptr(xds), _ptr(yds), _ptr(zds), imgXCenter, imgYCenter,
+                         imgZCenter, _ptr(hangs), _ptr(hzPos), PN, XN, YN, ZN, _ptr(hvol), _ptr(hprj), dx, dz,
+                         None if m is None else m.ctypes.data, methodId, st.ctypes.data_as(C.POINTER(C.c_int)),
+                         gpuNum)
+    check_last()
+
+
+def geometry_struct(g: DD3Geometry):
+    """(ctypes ctlab_geometry, arrays kept alive) for a geometry record."""
+    keep = [_f32(a) for a in (g.xds, g.yds, g.zds, g.hangs, g.hzPos)]
+    geo = _lib.Geometry(g.x0, g.y0, g.z0, g.DNU, g.DNV, _ptr(keep[0]), _ptr(keep[1]), _ptr(keep[2]),
+                        g.imgXCenter, g.imgYCenter, g.imgZCenter, _ptr(keep[3]), _ptr(keep[4]), g.PN, g.XN, g.YN,
+                        g.ZN, g.dx, g.dz)
+    return geo, keep
+
+
+def slab_views(g: DD3Geometry, z0: int, z1: int) -> np.ndarray:
+    """Views whose rays can reach slices [z0, z1) (ctlab_slab_views, host only); the
+    others add exactly zero to the slab's backprojection."""
+    lib = load()
+    geo, keep = geometry_struct(g)
+    out = np.zeros(max(g.PN, 1), np.int32)
+    n = lib.ctlab_slab_views(C.byref(geo), z0, z1, out.ctypes.data_as(C.POINTER(C.c_int)), out.size)
+    if n < 0:
+        check(-n)
+    return out[:n].copy()
+
+
+def slab_geometry(g: DD3Geometry, z0: int, z1: int, views=None) -> DD3Geometry:
+    """Slices [z0, z1) of g's volume as a volume of their own (same columns, its
+    slices centred where they sit in g), seen by `views` (default: slab_views)."""
+    import dataclasses
+    if views is None:
+        views = slab_views(g, z0, z1)
+    szn = z1 - z0
+    cz = float(np.float32(float(g.imgZCenter) + (z0 + 0.5 * szn - 0.5 * g.ZN) * float(g.dz)))
+    return dataclasses.replace(g, ZN=szn, imgZCenter=cz, hangs=g.hangs[views].copy(), hzPos=g.hzPos[views].copy())
+
+
 def _require(a, dtype, n, name):
     if not isinstance(a, np.ndarray) or a.dtype != dtype or not a.flags.c_contiguous or a.size != n:
         raise CtlabError(_lib.CTLAB_ERR_INVALID_ARG,

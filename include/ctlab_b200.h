@@ -78,6 +78,32 @@ void DD3Back_gpu(float x0, float y0, float z0, int DNU, int DNV, float *xds, flo
                  float *hprj, float dx, float dz, unsigned char *mask, int gpunum,
                  int squared, int prjMode);
 
+/* One scan split over gpuNum GPUs of this process (GPU i = CUDA device i):
+ * GPU i projects the views [startPN[i], startPN[i+1]) of the whole volume,
+ * startPN[gpuNum] taken as PN (startPN[0] == 0, non-decreasing), into its
+ * block of hprj.  Replaces DD3Proj_multiGPU, src/DD3_GPU_Proj.h:138-141
+ * (same name, arguments and order; prjMode 0 only).  With the environment
+ * variable CTLAB_MULTIGPU_WRAP=1 a split larger than the visible devices
+ * wraps around them (part i on device i mod count, parts of one device in
+ * turn); otherwise gpuNum must not exceed the device count. */
+void DD3Proj_multiGPU(float x0, float y0, float z0, int DNU, int DNV, float *xds, float *yds,
+                      float *zds, float imgXCenter, float imgYCenter, float imgZCenter,
+                      float *hangs, float *hzPos, int PN, int XN, int YN, int ZN, float *hvol,
+                      float *hprj, float dx, float dz, unsigned char *mask, int prjMode,
+                      int *startPN, int gpuNum);
+
+/* GPU i backprojects the z slab [startVOL[i], startVOL[i+1]) of the volume
+ * (startVOL[gpuNum] taken as ZN, startVOL[0] == 0, non-decreasing) from the
+ * views whose rays can reach the slab (ctlab_slab_views), and writes the
+ * slab's slices of every voxel column of hvol.  Replaces DD3Back_multiGPU,
+ * src/DD3_GPU_Back.h:138-142 (methodId 0 only); the per-slab view range
+ * plays the part of getPrjIdxPair, src/utilities.cuh:503-532. */
+void DD3Back_multiGPU(float x0, float y0, float z0, int DNU, int DNV, float *xds, float *yds,
+                      float *zds, float imgXCenter, float imgYCenter, float imgZCenter,
+                      float *hangs, float *hzPos, int PN, int XN, int YN, int ZN, float *hvol,
+                      float *hprj, float dx, float dz, unsigned char *mask, int methodId,
+                      int *startVOL, int gpuNum);
+
 /* Status of the last call on this thread (CTLAB_OK or CTLAB_ERR_*), and its
  * message ("" after success).  New in this library: the reference ignores
  * CUDA errors or exits (src/utilities.cuh:63-76). */
@@ -141,6 +167,24 @@ int ctlab_back_views(ctlab_plan *plan, const int *h_views, int n, const float *d
  * workspace (the first step of ctlab_proj), for tests and timing. */
 int ctlab_volume_sat(ctlab_plan *plan, const float *d_vol, const unsigned char *d_mask,
                      void *stream);
+
+/* Views of the scan whose rays can reach the z slab [z0, z1) of the volume,
+ * in increasing order, into h_views (capacity cap); returns how many there
+ * are (also when more than cap), or minus a CTLAB_ERR_* code.  A ray of
+ * view p runs between the source (z0 + hzPos[p]) and a detector cell
+ * (zds + hzPos[p]); a view is kept when that z range, widened by one row
+ * pitch, meets the slab widened by one voxel.  The views left out add
+ * exactly zero to the slab's backprojection.  Host only.  The counterpart
+ * of getPrjIdxPair, src/utilities.cuh:503-532 (which assumes hzPos sorted;
+ * this test takes any order). */
+int ctlab_slab_views(const ctlab_geometry *geom, int z0, int z1, int *h_views, int cap);
+
+/* The two multi-GPU splits with a plan-style geometry and status return
+ * (DD3Proj_multiGPU / DD3Back_multiGPU call these). */
+int ctlab_proj_multi(const ctlab_geometry *geom, const float *hvol, float *hprj,
+                     const unsigned char *mask, const int *startPN, int gpuNum);
+int ctlab_back_multi(const ctlab_geometry *geom, const float *hprj, float *hvol,
+                     const unsigned char *mask, const int *startVOL, int gpuNum);
 
 /* Allocation-free form of ctlab_volume_sat, for callers that cannot
  * allocate device memory mid-reconstruction: systems that reserve their
