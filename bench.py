@@ -56,6 +56,7 @@ def parse():
                          "helical: projection and backprojection of a 512x512x1024 helical scan")
     ap.add_argument("--train-volumes", type=int, default=16, help="learned workload: training phantoms")
     ap.add_argument("--train-steps", type=int, default=3000, help="learned workload: Adam steps")
+    ap.add_argument("--held-out", type=int, default=8, help="learned workload: held-out phantoms evaluated")
     ap.add_argument("--cases", type=int, default=48,
                     help="batch workload: keep the first N of the 48 cases (a profiling case)")
     ap.add_argument("--recon-iters", type=int, default=0,
@@ -646,10 +647,11 @@ def run_learned(args):
     noise I0 = 1e5.  Training pairs: for each seeded random-ellipsoid phantom, the
     2-iteration and the 30-iteration OS-SART images (24 subsets) of its noisy
     projections; 128 slice pairs per phantom.  The CNN trains with the library's own
-    kernels.  On a held-out phantom: plain = 30 OS-SART iterations from zero (residual
-    R30, device time T30); learned = 2 iterations + the CNN + the fewest further
-    iterations whose residual reaches R30.  Times are CUDA-event device times of the
-    solver calls; residual evaluations happen in separate, untimed passes."""
+    kernels.  On each of --held-out phantoms (seeds 7, 8, ...): plain = 30 OS-SART
+    iterations from zero (residual R30, device time T30); learned = 2 iterations + the
+    CNN + the fewest further iterations whose residual reaches R30; the line reports
+    every phantom and the median and worst time ratio.  Times are CUDA-event device
+    times of the solver calls; residual evaluations happen in separate, untimed passes."""
     import torch
 
     import ctlab_b200 as cb
@@ -710,52 +712,66 @@ def run_learned(args):
     t_train = time.perf_counter() - t0
     net.check_kernels()
 
-    truth, meas = scan(7)
-    clk = ClockSampler(local).__enter__()
-    # plain: 30 iterations from zero
-    x = torch.zeros_like(truth)
-    t30 = event_ms(lambda: plan.os_sart(x, meas, os_num=OS, iter_num=IT))
-    xr = torch.zeros_like(truth)
-    res_plain = plan.os_sart(xr, meas, os_num=OS, iter_num=IT, residuals=True)
-    r30 = float(res_plain[-1])
-    rmse_plain = float(torch.sqrt(torch.mean((x - truth) ** 2)))
-    # learned: 2 iterations, the network, then iterations until the residual reaches R30
-    xl = torch.zeros_like(truth)
-    t2 = event_ms(lambda: plan.os_sart(xl, meas, os_num=OS, iter_num=2))
-    xw = torch.zeros_like(truth)
-    # one untimed pass first: the first inference after training pays host-side
+    # one untimed inference first: the first inference after training pays host-side
     # start-up (allocator, first batch-16 shapes) that grows with the training run
-    net.predict_volume(xl, SCALE, torch.empty_like(xl))
-    tcnn = event_ms(lambda: net.predict_volume(xl, SCALE, xw))
-    net.check_kernels()
-    rmse_warm = float(torch.sqrt(torch.mean((xw - truth) ** 2)))
-    xc = xw.clone()
-    res_cont = plan.os_sart(xc, meas, os_num=OS, iter_num=IT, residuals=True)
-    hits = [k + 1 for k, r in enumerate(res_cont) if r <= r30]
-    k = hits[0] if hits else None
-    tk = 0.0
-    xk = xw.clone()
-    if k:
-        tk = event_ms(lambda: plan.os_sart(xk, meas, os_num=OS, iter_num=k))
-    rmse_learned = float(torch.sqrt(torch.mean((xk - truth) ** 2)))
+    _, warm_meas = scan(6)
+    xw0 = torch.zeros(g.vol_shape, dtype=torch.float32, device="cuda")
+    plan.os_sart(xw0, warm_meas, os_num=OS, iter_num=2)
+    net.predict_volume(xw0, SCALE, torch.empty_like(xw0))
+    del warm_meas, xw0
+
+    def held_out(seed):
+        truth, meas = scan(seed)
+        # plain: 30 iterations from zero
+        x = torch.zeros_like(truth)
+        t30 = event_ms(lambda: plan.os_sart(x, meas, os_num=OS, iter_num=IT))
+        xr = torch.zeros_like(truth)
+        res_plain = plan.os_sart(xr, meas, os_num=OS, iter_num=IT, residuals=True)
+        r30 = float(res_plain[-1])
+        rmse_plain = float(torch.sqrt(torch.mean((x - truth) ** 2)))
+        # learned: 2 iterations, the network, then iterations until the residual reaches R30
+        xl = torch.zeros_like(truth)
+        t2 = event_ms(lambda: plan.os_sart(xl, meas, os_num=OS, iter_num=2))
+        xw = torch.zeros_like(truth)
+        tcnn = event_ms(lambda: net.predict_volume(xl, SCALE, xw))
+        net.check_kernels()
+        rmse_warm = float(torch.sqrt(torch.mean((xw - truth) ** 2)))
+        xc = xw.clone()
+        res_cont = plan.os_sart(xc, meas, os_num=OS, iter_num=IT, residuals=True)
+        hits = [k + 1 for k, r in enumerate(res_cont) if r <= r30]
+        k = hits[0] if hits else None
+        tk = 0.0
+        xk = xw.clone()
+        if k:
+            tk = event_ms(lambda: plan.os_sart(xk, meas, os_num=OS, iter_num=k))
+        rmse_learned = float(torch.sqrt(torch.mean((xk - truth) ** 2)))
+        t_learned = t2 + tcnn + tk
+        return {"seed": seed, "plain_ms": t30, "residual_30": r30, "rmse_plain": rmse_plain,
+                "os_sart_2_ms": t2, "cnn_ms": tcnn, "continued_iterations": k, "continued_ms": tk,
+                "learned_ms": t_learned if k else None, "residual_after_cnn": float(res_cont[0]),
+                "rmse_after_cnn": rmse_warm, "rmse_learned": rmse_learned,
+                "time_ratio": (t_learned / t30) if k else None}
+
+    clk = ClockSampler(local).__enter__()
+    evals = [held_out(seed) for seed in range(7, 7 + max(1, args.held_out))]
     clk.__exit__(None, None, None)
-    x2_only = torch.zeros_like(truth)
-    plan.os_sart(x2_only, meas, os_num=OS, iter_num=2)
-    rmse_2 = float(torch.sqrt(torch.mean((x2_only - truth) ** 2)))
-    t_learned = t2 + tcnn + tk
+    ratios = [e["time_ratio"] for e in evals]
+    reached = [r for r in ratios if r is not None]
     line = {"metric": "learned warm start: time to the plain 30-iteration OS-SART residual",
             "workload": "learned_warm_start_256x256x128_720v_384x128", "n_gpus": 1,
             "data": "synthetic (seeded random-ellipsoid phantoms, Poisson noise I0=1e5)",
             "network": "2.5D residual CNN, 5 slices in, 8 conv3x3 layers of 64 channels, BF16 weights / FP32 accumulate",
             "training": {"volumes": args.train_volumes, "slice_pairs": args.train_volumes * g.ZN,
                          "steps": args.train_steps, "batch_slices": 8, "data_s": t_data, "train_s": t_train,
-                         "loss_first": float(np.mean(losses[:20])), "loss_last": float(np.mean(losses[-20:]))},
-            "plain": {"iterations": IT, "ms": t30, "residual": r30, "rmse": rmse_plain},
-            "learned": {"os_sart_2_ms": t2, "cnn_ms": tcnn, "continued_iterations": k, "continued_ms": tk,
-                        "ms": t_learned if k else None, "residual_after_cnn": float(res_cont[0]),
-                        "rmse_2_iterations": rmse_2, "rmse_after_cnn": rmse_warm, "rmse": rmse_learned},
-            "time_ratio": (t_learned / t30) if k else None, "target_ratio": 0.5,
-            "clocks": clk.summary()}
+                         "loss_first": float(np.mean(losses[:20])), "loss_last": float(np.mean(losses[-20:])),
+                         "deviation": f"{args.train_volumes} method-generated volume pairs ({args.train_volumes * g.ZN} "
+                                      "slice pairs), not 2000 volume pairs: 2000 x 30 OS-SART iterations would take "
+                                      "about 45 min of GPU time per run"},
+            "held_out": evals, "held_out_phantoms": len(evals),
+            "reached_plain_residual": len(reached),
+            "time_ratio_median": float(np.median(reached)) if reached else None,
+            "time_ratio_worst": float(max(reached)) if len(reached) == len(evals) else None,
+            "target_ratio": 0.5, "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
     plan.close()
 

@@ -30,7 +30,9 @@
 // the issue of view l+2's copy.  Views whose footprint exceeds a stage read P
 // from global memory.  Epilogue: in-plane mask and optionally the OS-SART
 // update x = (x + lambda * acc/colSum) * mask.
+#include <algorithm>
 #include <climits>
+#include <cstdlib>
 #include <cmath>
 #include <type_traits>
 #include <utility>
@@ -44,10 +46,11 @@ namespace {
 
 constexpr int kB = 8;                 // brick edge (voxel columns)
 constexpr int kCols = kB * kB;        // 64 columns per CTA
-constexpr int kZS = 8;                // z segments per column
-constexpr int kThreads = kCols * kZS; // 512
+// z segments per column ZS (template parameter): 8 (512 threads, KSEG up to
+// 32 accumulators a thread) or 16 (1024 threads, twice the warps to hide the
+// shared-memory latency of phase B, at most 64 registers a thread)
 constexpr size_t kSmemPerCta = 200 * 1024; // one CTA per SM
-constexpr size_t kStaticSmem = 6 * 1024;
+constexpr size_t kStaticSmem = 20 * 1024;
 constexpr int kGeo = 4;               // geometry slots (views l .. l+3)
 
 __device__ __forceinline__ float lds_f32(uint32_t addr)
@@ -110,14 +113,24 @@ __device__ __forceinline__ double cross2(double ax, double ay, double bx, double
     return ax * by - ay * bx;
 }
 
+// Phase-A set-up of one column for one view, computed two views ahead by
+// 64 threads instead of by each of the column's ZS phase-A threads: byte
+// offsets of the strip's staged P rows from the stage origin (a, b and up to
+// three whole cells between), the strip weights and the whole-cell count.
+struct ASet {
+    uint32_t off[5];
+    float wa, wb, wm[3];
+    int nm, pad;
+};
+
 __device__ __forceinline__ double u_of(const DevView &V, double px, double py)
 {
     const double dpx = px - V.Sx, dpy = py - V.Sy;
     return cross2(V.Sx - V.B0x, V.Sy - V.B0y, dpx, dpy) / cross2(V.Ex, V.Ey, dpx, dpy);
 }
 
-template <int KSEG, int VPT, bool ZSKIP>
-__global__ void __launch_bounds__(kThreads, 1) dd3_back_t_kernel(BackArgs a, int es2, int rmax)
+template <int ZS, int KSEG, int VPT, bool ZSKIP>
+__global__ void __launch_bounds__(kCols * ZS, 1) dd3_back_t_kernel(BackArgs a, int es2, int rmax)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     const int vp = a.vp; // P row pitch (floats, multiple of 4)
@@ -129,13 +142,14 @@ __global__ void __launch_bounds__(kThreads, 1) dd3_back_t_kernel(BackArgs a, int
     __shared__ float s_V0[kGeo][kCols], s_V1[kGeo][kCols];
     __shared__ int s_xdrv[kGeo];
     __shared__ int s_cov[kGeo][2]; // the view's cone meets this CTA's z range (per column half)
+    __shared__ __align__(16) ASet s_aset[kGeo][kCols];
 
     const int tid = threadIdx.x;
     const int bx0 = blockIdx.x * kB, by0 = blockIdx.y * kB;
     const int col = tid & (kCols - 1), zs = tid / kCols;
     const int cx = col & (kB - 1), cy = col / kB;
     const int x = bx0 + cx, y = by0 + cy;
-    const int k0 = blockIdx.z * (kZS * KSEG) + zs * KSEG;
+    const int k0 = blockIdx.z * (ZS * KSEG) + zs * KSEG;
     const int DNU = a.DNU, DNV = a.DNV, ZN = a.ZN;
     // the list positions this CTA visits: all, or (ZSKIP) the range of views
     // whose cone can meet its z block
@@ -145,17 +159,15 @@ __global__ void __launch_bounds__(kThreads, 1) dd3_back_t_kernel(BackArgs a, int
         lb = r.x;
         n = max(r.y - r.x, 0);
     }
-    const double dx = a.dx;
-    const double x_lo = a.x_c0 - 0.5 * dx, y_lo = a.y_c0 - 0.5 * dx;
+    // geometry constants are re-read from the kernel parameters (constant
+    // bank) where they are used, so they hold no registers across the loop
     const DetTable t = det_table_layout(DNU, DNV);
-    const double zb0_local = a.det[t.off_bz];
+    __shared__ double s_zb0; // local z of the detector's first row boundary
+    if (tid == 0) s_zb0 = a.det[t.off_bz];
     const bool in_vol = (x < a.XN) && (y < a.YN);
-    const float *Pall = a.pv;
-    const long long pstride = (long long)DNU * vp;
     const float DNVf = (float)DNV;
-    const double inv_n = 1.0 / (a.dzb * DNV), dz_n = a.dz * inv_n; // detector rows, normalised by DNV
     // z boundaries this CTA's phase B samples (its segments' k0 .. k0 + KSEG)
-    const float kz_lo = (float)(blockIdx.z * (kZS * KSEG)), kz_hi = kz_lo + (float)(kZS * KSEG);
+    const float kz_lo = (float)(blockIdx.z * (ZS * KSEG)), kz_hi = kz_lo + (float)(ZS * KSEG);
 
     if (tid == 0) {
         mbar_init(&s_bar[0], 1);
@@ -174,23 +186,24 @@ __global__ void __launch_bounds__(kThreads, 1) dd3_back_t_kernel(BackArgs a, int
             const int r = tid / (kB + 1), q = tid - r * (kB + 1);
             double px, py;
             if (!V.xdrv) {
-                px = x_lo + (double)(bx0 + q) * dx;
-                py = a.y_c0 + (double)(by0 + r) * dx;
+                px = a.x_c0 + ((double)(bx0 + q) - 0.5) * a.dx;
+                py = a.y_c0 + (double)(by0 + r) * a.dx;
             } else {
-                px = a.x_c0 + (double)(bx0 + r) * dx;
-                py = y_lo + (double)(by0 + q) * dx;
+                px = a.x_c0 + (double)(bx0 + r) * a.dx;
+                py = a.y_c0 + ((double)(by0 + q) - 0.5) * a.dx;
             }
             s_u[sl][r][q] = u_of(V, px, py);
             if (tid == 0) s_xdrv[sl] = V.xdrv;
         } else if (tid >= 128 && tid < 128 + kCols) {
             const int c = tid - 128;
-            const double pcx = a.x_c0 + (double)(bx0 + (c & (kB - 1))) * dx;
-            const double pcy = a.y_c0 + (double)(by0 + c / kB) * dx;
+            const double pcx = a.x_c0 + (double)(bx0 + (c & (kB - 1))) * a.dx;
+            const double pcy = a.y_c0 + (double)(by0 + c / kB) * a.dx;
             const double tc = cross2(V.B0x - V.Sx, V.B0y - V.Sy, V.Ex, V.Ey) /
                               cross2(pcx - V.Sx, pcy - V.Sy, V.Ex, V.Ey);
-            const double zb0 = zb0_local + V.zP;
+            const double zb0 = s_zb0 + V.zP;
             // z boundary k' -> detector row coordinate v = V0 + V1 k', stored / DNV
-            const float V1 = (float)(tc * dz_n), V0 = (float)((V.Sz + tc * (a.z_lo - V.Sz) - zb0) * inv_n);
+            const double inv_n = 1.0 / (a.dzb * a.DNV); // detector rows, normalised by DNV
+            const float V1 = (float)(tc * a.dz * inv_n), V0 = (float)((V.Sz + tc * (a.z_lo - V.Sz) - zb0) * inv_n);
             s_V1[sl][c] = V1;
             s_V0[sl][c] = V0;
             if (ZSKIP) {
@@ -222,16 +235,68 @@ __global__ void __launch_bounds__(kThreads, 1) dd3_back_t_kernel(BackArgs a, int
         s_rows[b] = meets ? (fits ? rows : 0) : -1; // -1: the view misses the brick
         mbar_arrive_expect_tx(&s_bar[b], fits ? (uint32_t)(4 * rows * vp) : 0u);
         if (fits)
-            bulk_copy_g2s(pbuf + (size_t)b * rmax * vp, Pall + (long long)(lb + l) * pstride + (long long)lo * vp,
+            bulk_copy_g2s(pbuf + (size_t)b * rmax * vp, a.pv + ((long long)(lb + l) * DNU + lo) * vp,
                           (uint32_t)(4 * rows * vp), &s_bar[b]);
     };
 
+    // phase-A set-up of list entry l into slot l % kGeo (threads 256..319,
+    // one per column): the same staging origin as issue(l), from the same
+    // corner boundaries
+    auto setup = [&](int l) {
+        if (l >= n || tid < 256 || tid >= 256 + kCols) return;
+        const int c = tid - 256, sl = l % kGeo;
+        const int ccx = c & (kB - 1), ccy = c / kB;
+        const double u0 = s_u[sl][0][0], u1 = s_u[sl][0][kB], u2 = s_u[sl][kB - 1][0], u3 = s_u[sl][kB - 1][kB];
+        const double umin = fmin(fmax(fmin(fmin(u0, u1), fmin(u2, u3)), 0.0), (double)(DNU - 1));
+        const double umax = fmin(fmax(fmax(fmax(u0, u1), fmax(u2, u3)), 0.0), (double)(DNU - 1));
+        const int lo = max((int)umin - 1, 0), rows = min((int)umax + 2, DNU - 1) - lo + 1;
+        const int xd = s_xdrv[sl];
+        const double ua = xd ? s_u[sl][ccx][ccy] : s_u[sl][ccy][ccx];
+        const double ub = xd ? s_u[sl][ccx][ccy + 1] : s_u[sl][ccy][ccx + 1];
+        const double uca = fmin(fmax(ua, 0.0), (double)DNU), ucb = fmin(fmax(ub, 0.0), (double)DNU);
+        const int ia = min((int)uca, DNU - 1), ib = min((int)ucb, DNU - 1);
+        const float fa = (float)(uca - ia), fb = (float)(ucb - ib);
+        const float sg = ((ub - ua > 0) ? 1.f : -1.f) * ((s_V1[sl][c] > 0.f) ? 1.f : -1.f);
+        const int dc = ib - ia;
+        float wa, wb;
+        if (dc == 0) {
+            wa = fb - fa;
+            wb = 0.f;
+        } else if (dc > 0) {
+            wa = 1.f - fa;
+            wb = fb;
+        } else {
+            wa = -fa;
+            wb = fb - 1.f;
+        }
+        const int nm = max(abs(dc) - 1, 0), first = min(ia, ib) + 1;
+        const float wm = dc > 0 ? sg : -sg;
+        const uint32_t vp4 = 4u * (uint32_t)a.vp;
+        auto row = [&](int u) { return (uint32_t)min(max(u - lo, 0), max(rows - 1, 0)) * vp4; };
+        ASet st;
+        st.off[0] = row(ia);
+        st.off[1] = row(ib);
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            st.off[2 + m] = row(min(first + m, max(ia, ib)));
+            st.wm[m] = m < nm ? wm : 0.f;
+        }
+        st.wa = wa * sg;
+        st.wb = wb * sg;
+        st.nm = nm;
+        st.pad = 0;
+        s_aset[sl][c] = st;
+    };
+
+    __syncthreads(); // s_zb0 visible
     geometry(0);
     geometry(1);
     geometry(2);
     __syncthreads(); // barrier init and geometry visible
     issue(0);
     issue(1);
+    setup(0);
+    setup(1);
     __syncthreads();
 
     float acc[KSEG];
@@ -240,7 +305,7 @@ __global__ void __launch_bounds__(kThreads, 1) dd3_back_t_kernel(BackArgs a, int
     bool timed_out = false;
     const uint32_t E2_addr = smem_addr(E2);
     // phase A: kAPh threads per column, each a run of vpt consecutive rows
-    constexpr int kAPh = kThreads / kCols;
+    constexpr int kAPh = ZS;
     const int ac = tid / kAPh, aph = tid % kAPh;
     const int acx = ac & (kB - 1), acy = ac / kB;
     const int i0 = aph * VPT; // this thread's entries i0 .. i0+VPT-1 (kAPh*VPT > DNV)
@@ -248,19 +313,28 @@ __global__ void __launch_bounds__(kThreads, 1) dd3_back_t_kernel(BackArgs a, int
     for (int li = 0; li < n; ++li) {
         const int b = li & 1, ls = li % kGeo;
         const int ulo = s_ulo[b], rows = s_rows[b];
-        if (!mbar_wait(&s_bar[b], (uint32_t)((li >> 1) & 1))) timed_out = true;
+        // warp-uniform, so the warp collectives of phase A stay converged
+        if (__any_sync(0xffffffffu, !mbar_wait(&s_bar[b], (uint32_t)((li >> 1) & 1)))) timed_out = true;
         const int xdrv = s_xdrv[ls];
         float2 *E = E2 + (size_t)b * kCols * es2; // double buffered: B(li) overlaps A(li+1)
 
         // ---- A: (E_c(i), E_c(i+1) - E_c(i)) for i in [0, DNV], E_c(DNV+1) = E_c(DNV) ----
-        if (!timed_out && (!ZSKIP || rows >= 0)) {
+        // the thread's column strip for this view, recomputed from s_u (the
+        // paths the hoisted set-up does not cover)
+        struct Strip {
+            int ia, ib, nm, first;
+            float wa, wb, wm;
+        };
+        auto strip = [&]() {
+            Strip st;
             const double ua = xdrv ? s_u[ls][acx][acy] : s_u[ls][acy][acx];
             const double ub = xdrv ? s_u[ls][acx][acy + 1] : s_u[ls][acy][acx + 1];
             const double uca = fmin(fmax(ua, 0.0), (double)DNU), ucb = fmin(fmax(ub, 0.0), (double)DNU);
-            const int ia = min((int)uca, DNU - 1), ib = min((int)ucb, DNU - 1);
-            const float fa = (float)(uca - ia), fb = (float)(ucb - ib);
+            st.ia = min((int)uca, DNU - 1);
+            st.ib = min((int)ucb, DNU - 1);
+            const float fa = (float)(uca - st.ia), fb = (float)(ucb - st.ib);
             const float sg = ((ub - ua > 0) ? 1.f : -1.f) * ((s_V1[ls][ac] > 0.f) ? 1.f : -1.f);
-            const int dc = ib - ia;
+            const int dc = st.ib - st.ia;
             float wa, wb;
             if (dc == 0) {
                 wa = fb - fa;
@@ -272,61 +346,67 @@ __global__ void __launch_bounds__(kThreads, 1) dd3_back_t_kernel(BackArgs a, int
                 wa = -fa;
                 wb = fb - 1.f;
             }
-            wa *= sg;
-            wb *= sg;
-            // whole cells strictly between a and b; the warp runs its widest
-            // column's count, the others with weight 0
-            const int nm = max(abs(dc) - 1, 0), first = min(ia, ib) + 1;
-            const int nmax = __reduce_max_sync(0xffffffffu, nm);
-            const float wm = dc > 0 ? sg : -sg;
-            if (rows > 0) {
-                // staged rows: 32-bit shared addresses, row u at pbase + (u - ulo) * vp4;
-                // the pitch covers i0+VPT, and entries past DNV repeat the total
+            st.wa = wa * sg;
+            st.wb = wb * sg;
+            // whole cells strictly between a and b
+            st.nm = max(abs(dc) - 1, 0);
+            st.first = min(st.ia, st.ib) + 1;
+            st.wm = dc > 0 ? sg : -sg;
+            return st;
+        };
+
+        if (!timed_out && rows > 0) {
+            // staged rows, set-up from s_aset: 32-bit shared addresses, row u at
+            // pbase + (u - ulo) * vp4; the pitch covers i0+VPT, and entries past
+            // DNV repeat the total
+            const uint4 q0 = *reinterpret_cast<const uint4 *>(&s_aset[ls][ac].off[0]);
+            const uint4 q1 = *reinterpret_cast<const uint4 *>(&s_aset[ls][ac].off[4]);
+            const uint4 q2 = *reinterpret_cast<const uint4 *>(&s_aset[ls][ac].wm[1]);
+            const uint32_t pbase = smem_addr(pbuf + (size_t)b * rmax * vp) + 4u * (uint32_t)i0;
+            const uint32_t pa = pbase + q0.x, pb = pbase + q0.y;
+            const uint32_t pm[3] = {pbase + q0.z, pbase + q0.w, pbase + q1.x};
+            const float wa = __uint_as_float(q1.y), wb = __uint_as_float(q1.z);
+            const float wmv[3] = {__uint_as_float(q1.w), __uint_as_float(q2.x), __uint_as_float(q2.y)};
+            // the warp runs its widest column's whole-cell count, the others with weight 0
+            const int nmax = (int)__reduce_max_sync(0xffffffffu, q2.z);
+            const uint32_t eout = E2_addr + 8u * (uint32_t)((b * kCols + ac) * es2 + i0);
+            switch (nmax) {
+            case 0: phase_a_run<VPT, 0>(pa, pb, pm, wmv, wa, wb, eout); break;
+            case 1: phase_a_run<VPT, 1>(pa, pb, pm, wmv, wa, wb, eout); break;
+            case 2: phase_a_run<VPT, 2>(pa, pb, pm, wmv, wa, wb, eout); break;
+            case 3: phase_a_run<VPT, 3>(pa, pb, pm, wmv, wa, wb, eout); break;
+            default: {
+                // cells much wider than voxels: the whole cells by a loop
+                const Strip st = strip();
                 const uint32_t vp4 = 4u * (uint32_t)vp;
-                const uint32_t pbase = smem_addr(pbuf + (size_t)b * rmax * vp) + 4u * (uint32_t)i0;
-                auto row = [&](int u) { return pbase + (uint32_t)min(max(u - ulo, 0), rows - 1) * vp4; };
-                const uint32_t pa = row(ia), pb = row(ib);
-                const uint32_t eout = E2_addr + 8u * (uint32_t)((b * kCols + ac) * es2 + i0);
-                uint32_t pm[3];
-                float wmv[3];
-#pragma unroll
-                for (int m = 0; m < 3; ++m) {
-                    pm[m] = row(min(first + m, max(ia, ib)));
-                    wmv[m] = m < nm ? wm : 0.f;
-                }
-                switch (nmax) {
-                case 0: phase_a_run<VPT, 0>(pa, pb, pm, wmv, wa, wb, eout); break;
-                case 1: phase_a_run<VPT, 1>(pa, pb, pm, wmv, wa, wb, eout); break;
-                case 2: phase_a_run<VPT, 2>(pa, pb, pm, wmv, wa, wb, eout); break;
-                case 3: phase_a_run<VPT, 3>(pa, pb, pm, wmv, wa, wb, eout); break;
-                default: {
-                    // cells much wider than voxels: the whole cells by a loop
-                    float2 *Ec = E + ac * es2;
-                    float e = 0.f;
-                    for (int j = 0; j <= VPT; ++j) {
-                        const uint32_t o = 4u * (uint32_t)j;
-                        float en = fmaf(wb, lds_f32(pb + o), wa * lds_f32(pa + o));
-                        for (int m = 0; m < nm; ++m) en = fmaf(wm, lds_f32(row(first + m) + o), en);
-                        if (j > 0) Ec[i0 + j - 1] = make_float2(e, en - e);
-                        e = en;
-                    }
-                }
-                }
-            } else {
-                // footprint wider than a stage: P from global memory
-                const float *Pg = Pall + (long long)(lb + li) * pstride;
+                const uint32_t sbase = smem_addr(pbuf + (size_t)b * rmax * vp) + 4u * (uint32_t)i0;
+                auto row = [&](int u) { return sbase + (uint32_t)min(max(u - ulo, 0), rows - 1) * vp4; };
                 float2 *Ec = E + ac * es2;
-                auto eval = [&](int i) {
-                    float e = fmaf(wb, __ldg(Pg + (size_t)ib * vp + i), wa * __ldg(Pg + (size_t)ia * vp + i));
-                    for (int m = 0; m < nm; ++m) e = fmaf(wm, __ldg(Pg + (size_t)(first + m) * vp + i), e);
-                    return e;
-                };
-                float e = eval(i0);
-                for (int j = 0; j < VPT; ++j) {
-                    const float en = eval(i0 + j + 1);
-                    Ec[i0 + j] = make_float2(e, en - e);
+                float e = 0.f;
+                for (int j = 0; j <= VPT; ++j) {
+                    const uint32_t o = 4u * (uint32_t)j;
+                    float en = fmaf(st.wb, lds_f32(row(st.ib) + o), st.wa * lds_f32(row(st.ia) + o));
+                    for (int m = 0; m < st.nm; ++m) en = fmaf(st.wm, lds_f32(row(st.first + m) + o), en);
+                    if (j > 0) Ec[i0 + j - 1] = make_float2(e, en - e);
                     e = en;
                 }
+            }
+            }
+        } else if (!timed_out && (!ZSKIP || rows >= 0)) {
+            // footprint wider than a stage: P from global memory
+            const Strip st = strip();
+            const float *Pg = a.pv + (long long)(lb + li) * DNU * vp;
+            float2 *Ec = E + ac * es2;
+            auto eval = [&](int i) {
+                float e = fmaf(st.wb, __ldg(Pg + (size_t)st.ib * vp + i), st.wa * __ldg(Pg + (size_t)st.ia * vp + i));
+                for (int m = 0; m < st.nm; ++m) e = fmaf(st.wm, __ldg(Pg + (size_t)(st.first + m) * vp + i), e);
+                return e;
+            };
+            float e = eval(i0);
+            for (int j = 0; j < VPT; ++j) {
+                const float en = eval(i0 + j + 1);
+                Ec[i0 + j] = make_float2(e, en - e);
+                e = en;
             }
         }
         __syncthreads();
@@ -334,6 +414,7 @@ __global__ void __launch_bounds__(kThreads, 1) dd3_back_t_kernel(BackArgs a, int
         // ---- stage view li+2 into the buffer just consumed; geometry of li+3 ----
         issue(li + 2);
         geometry(li + 3);
+        setup(li + 2);
 
         // ---- phase B: voxels ----
         if (in_vol && !timed_out && (!ZSKIP || rows >= 0)) {
@@ -405,15 +486,29 @@ __global__ void __launch_bounds__(256) pv_kernel(PrjIn in, long long ncols, int 
     for (int v = DNV + 1 + lane; v < vp; v += 32) o[v] = (float)carry;
 }
 
-// Rows of E per phase-A thread: kAPh * VPT > DNV, from a few compiled sizes.
-int vpt_of(int DNV)
+// Rows of E per phase-A thread with ZS threads per column: ZS * VPT > DNV,
+// from a few compiled sizes.
+int vpt_of(int DNV, int zs)
 {
-    const int need = (DNV + 1 + kThreads / kCols - 1) / (kThreads / kCols);
+    const int need = (DNV + 1 + zs - 1) / zs;
     for (int v : {2, 5, 9, 17, 33})
         if (v >= need) return v;
     return 0;
 }
-int e_pitch(int DNV) { return ((kThreads / kCols) * vpt_of(DNV)) | 1; }
+int e_pitch(int DNV, int zs) { return (zs * vpt_of(DNV, zs)) | 1; }
+// the largest (E, dE) pitch over the two block shapes
+int e_pitch_max(int DNV) { return std::max(e_pitch(DNV, 8), e_pitch(DNV, 16)); }
+
+// z segments per column: 16 (1024 threads) unless CTLAB_BACKT_ZS=8 selects
+// the 512-thread shape; both give the same results.
+int back_t_zs()
+{
+    static const int zs = [] {
+        const char *e = std::getenv("CTLAB_BACKT_ZS");
+        return (e && std::atoi(e) == 8) ? 8 : 16;
+    }();
+    return zs;
+}
 
 size_t dyn_smem(int rmax, int vp, int es2)
 {
@@ -476,50 +571,65 @@ __global__ void __launch_bounds__(256) zrange_kernel(BackArgs a, int zblk, int2 
     }
 }
 
-template <int KSEG, int VPT, bool ZSKIP>
+template <int ZS, int KSEG, int VPT, bool ZSKIP>
 cudaError_t launch_k(const BackArgs &a, cudaStream_t s)
 {
-    const int es2 = e_pitch(a.DNV); // (E, dE) pairs per column, odd pitch
+    const int es2 = e_pitch(a.DNV, ZS); // (E, dE) pairs per column, odd pitch
     const size_t sm = dyn_smem(a.rmax, a.vp, es2);
-    auto kern = dd3_back_t_kernel<KSEG, VPT, ZSKIP>;
+    auto kern = dd3_back_t_kernel<ZS, KSEG, VPT, ZSKIP>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    dim3 grid((a.XN + kB - 1) / kB, (a.YN + kB - 1) / kB, (a.ZN + kZS * KSEG - 1) / (kZS * KSEG));
+    dim3 grid((a.XN + kB - 1) / kB, (a.YN + kB - 1) / kB, (a.ZN + ZS * KSEG - 1) / (ZS * KSEG));
     if (ZSKIP && a.zrange) {
-        zrange_kernel<<<grid.z, 256, 0, s>>>(a, kZS * KSEG, a.zrange);
+        zrange_kernel<<<grid.z, 256, 0, s>>>(a, ZS * KSEG, a.zrange);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
-    kern<<<grid, kThreads, sm, s>>>(a, es2, a.rmax);
+    kern<<<grid, kCols * ZS, sm, s>>>(a, es2, a.rmax);
     return cudaGetLastError();
 }
 
-// Segment length by ZN; volumes of several z blocks (and helical scans with
-// 256-voxel blocks) test each view against each CTA's z range and skip the
-// views whose cone misses it.
-template <int VPT>
+// Segment length by ZN (z blocks of 256 voxels at most); volumes of several
+// z blocks (and helical scans) test each view against each CTA's z range and
+// skip the views whose cone misses it.  512 threads: segments up to 32
+// voxels; 1024 threads: up to 16.
+template <int ZS, int VPT>
 cudaError_t launch_z(const BackArgs &a, cudaStream_t s)
 {
-    if (a.ZN <= kZS * 4) return launch_k<4, VPT, false>(a, s);
-    if (a.ZN <= kZS * 8) return launch_k<8, VPT, false>(a, s);
-    if (a.ZN <= kZS * 16) return launch_k<16, VPT, false>(a, s);
-    if (a.zskip || a.ZN > kZS * 32) return launch_k<32, VPT, true>(a, s);
-    return launch_k<32, VPT, false>(a, s);
+    constexpr int KMAX = 256 / ZS;
+    if (a.ZN <= ZS * 4) return launch_k<ZS, 4, VPT, false>(a, s);
+    if (a.ZN <= ZS * 8) return launch_k<ZS, 8, VPT, false>(a, s);
+    if (ZS * 16 < 256 && a.ZN <= ZS * 16) return launch_k<ZS, 16, VPT, false>(a, s);
+    if (a.zskip || a.ZN > 256) return launch_k<ZS, KMAX, VPT, true>(a, s);
+    return launch_k<ZS, KMAX, VPT, false>(a, s);
+}
+
+template <int ZS>
+cudaError_t launch_vpt(const BackArgs &a, cudaStream_t s)
+{
+    switch (vpt_of(a.DNV, ZS)) {
+    case 2: return launch_z<ZS, 2>(a, s);
+    case 5: return launch_z<ZS, 5>(a, s);
+    case 9: return launch_z<ZS, 9>(a, s);
+    case 17: return launch_z<ZS, 17>(a, s);
+    case 33: return launch_z<ZS, 33>(a, s);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 } // namespace
 
 bool back_t_supported(int DNV)
 {
-    if (vpt_of(DNV) == 0) return false;
-    return dyn_smem(2, back_t_pitch(DNV), e_pitch(DNV)) + kStaticSmem <= 227 * 1024;
+    if (vpt_of(DNV, 8) == 0 || vpt_of(DNV, 16) == 0) return false;
+    return dyn_smem(2, back_t_pitch(DNV), e_pitch_max(DNV)) + kStaticSmem <= 227 * 1024;
 }
 
 // P row pitch: DNV+1 prefixes, then the total repeated up to the last row a
 // phase-A run reads (kAPh * VPT), rounded to 16 bytes
 int back_t_pitch(int DNV)
 {
-    return (std::max(DNV + 2, (kThreads / kCols) * vpt_of(DNV) + 1) + 3) & ~3;
+    return (std::max(DNV + 2, std::max(8 * vpt_of(DNV, 8), 16 * vpt_of(DNV, 16)) + 1) + 3) & ~3;
 }
 
 // Staged P rows: the widest u footprint of any brick on the volume's outer
@@ -528,7 +638,7 @@ int back_t_pitch(int DNV)
 int back_t_staging_rows(const HostGeometry &g)
 {
     const int vp = back_t_pitch(g.DNV);
-    const int es2 = e_pitch(g.DNV);
+    const int es2 = e_pitch_max(g.DNV);
     const double x_c0 = g.cx - 0.5 * (g.XN - 1) * g.dx, y_c0 = g.cy - 0.5 * (g.YN - 1) * g.dx;
     const double x_lo = x_c0 - 0.5 * g.dx, y_lo = y_c0 - 0.5 * g.dx;
     const int nbx = (g.XN + kB - 1) / kB, nby = (g.YN + kB - 1) / kB;
@@ -580,14 +690,7 @@ cudaError_t launch_back_t(const BackArgs &a, cudaStream_t s, int *launches)
 {
     if (launches) ++*launches;
     if (a.n <= 0) return cudaSuccess;
-    switch (vpt_of(a.DNV)) {
-    case 2: return launch_z<2>(a, s);
-    case 5: return launch_z<5>(a, s);
-    case 9: return launch_z<9>(a, s);
-    case 17: return launch_z<17>(a, s);
-    case 33: return launch_z<33>(a, s);
-    default: return cudaErrorInvalidValue;
-    }
+    return back_t_zs() == 8 ? launch_vpt<8>(a, s) : launch_vpt<16>(a, s);
 }
 
 } // namespace ctlab

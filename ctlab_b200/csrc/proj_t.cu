@@ -68,7 +68,8 @@ struct TEntry {
 struct TSlice {
     int c_lo, k_lo, fits, nbox;
     float kz_lo, kz_hi;
-    int pad0, pad1;
+    float inv_span; // 1 / (kz_hi - kz_lo)
+    int pad1;
 };
 
 __device__ __forceinline__ float lds_f32(uint32_t addr)
@@ -91,17 +92,19 @@ __device__ __forceinline__ float zinterp(uint32_t pa, uint32_t RS4, float fz)
     return fmaf(fz, c1 - c0, c0);
 }
 
-// Staged slice address of the z-prefix row holding kz (clamped to the box),
-// and the fraction of kz past that row.  0 <= kz < 2^23, so adding 2^23
-// toward zero leaves floor(kz) in the mantissa bits; base folds in the box
-// origin and the 2^23 exponent bits.
-__device__ __forceinline__ uint32_t zrow_addr(float T, float e, float z0, float kzlo, float kzhi, uint32_t RS4,
-                                              uint32_t base, float &fz)
+// Staged slice address of the z-prefix row holding kz, clamped to the box
+// [kz_lo, kz_hi], and the fraction of kz past that row.  The caller passes
+// kz normalised to the box, vn = (kz - kz_lo) / span with span = kz_hi -
+// kz_lo, as vn = Tn e + z0n: one saturating FMA clamps, and the
+// round-toward-zero FMA adding 2^23 leaves floor(vn span) -- the row past
+// kz_lo -- in the mantissa bits; base folds in the box origin and the 2^23
+// exponent bits.
+__device__ __forceinline__ uint32_t zrow_addr(float Tn, float e, float z0n, float span, uint32_t RS4, uint32_t base,
+                                              float &fz)
 {
-    float kz = fmaf(T, e, z0);
-    kz = fminf(fmaxf(kz, kzlo), kzhi);
-    const float rr = __fadd_rz(kz, 8388608.f);
-    fz = kz - (rr - 8388608.f);
+    const float vn = __saturatef(fmaf(Tn, e, z0n));
+    const float rr = __fmaf_rz(vn, span, 8388608.f);
+    fz = fmaf(vn, span, 8388608.f - rr);
     return __float_as_uint(rr) * RS4 + base;
 }
 
@@ -110,7 +113,7 @@ __device__ __forceinline__ uint32_t zrow_addr(float T, float e, float z0, float 
 // F(row boundary) = wa Z(a) + wb Z(b); acc[r] += (F(r + 1) - F(r)) scale.
 template <int NR>
 __device__ __forceinline__ void rows_narrow(float (&acc)[NR], const TEntry &te, int dc, uint32_t e_addr, uint32_t base,
-                                            uint32_t RS4, float z0, float kzlo, float kzhi)
+                                            uint32_t RS4, float Tn, float z0n, float span)
 {
     const uint32_t dc4 = 4u * (uint32_t)dc;
     float prev = 0.f;
@@ -123,7 +126,7 @@ __device__ __forceinline__ void rows_narrow(float (&acc)[NR], const TEntry &te, 
             const int r = r4 + q;
             if (r > NR) break;
             float fz;
-            const uint32_t pa = zrow_addr(te.T, ev[q], z0, kzlo, kzhi, RS4, base, fz), pb = pa + dc4;
+            const uint32_t pa = zrow_addr(Tn, ev[q], z0n, span, RS4, base, fz), pb = pa + dc4;
             const float a0 = lds_f32(pa), a1 = lds_f32(pa + RS4);
             const float b0 = lds_f32(pb), b1 = lds_f32(pb + RS4);
             const float F = fmaf(te.wb, fmaf(fz, b1 - b0, b0), te.wa * fmaf(fz, a1 - a0, a0));
@@ -145,7 +148,7 @@ __device__ __forceinline__ float strip_weight(const TEntry &te, int i, int dc, i
 // voxel columns: one pass over the columns a .. a + M sgn(dc) per row.
 template <int NR, int M>
 __device__ __forceinline__ void rows_wide(float (&acc)[NR], const TEntry &te, int dc, uint32_t e_addr, uint32_t base,
-                                          uint32_t RS4, float z0, float kzlo, float kzhi)
+                                          uint32_t RS4, float Tn, float z0n, float span)
 {
     const int adc = dc < 0 ? -dc : dc;
     const int step4 = dc < 0 ? -4 : 4;
@@ -166,7 +169,7 @@ __device__ __forceinline__ void rows_wide(float (&acc)[NR], const TEntry &te, in
             const int r = r4 + q;
             if (r > NR) break;
             float fz;
-            const uint32_t pa = zrow_addr(te.T, ev[q], z0, kzlo, kzhi, RS4, base, fz);
+            const uint32_t pa = zrow_addr(Tn, ev[q], z0n, span, RS4, base, fz);
             float F = w[0] * zinterp(pa, RS4, fz);
 #pragma unroll
             for (int i = 1; i <= M; ++i) F = fmaf(w[i], zinterp(pa + off[i], RS4, fz), F);
@@ -366,7 +369,8 @@ __device__ __forceinline__ void proj_t_tile(const ProjArgs &a, const CUtensorMap
                 in.nbox = nbox;
                 in.kz_lo = fits ? (float)k_lo : 0.f;
                 in.kz_hi = fits ? (float)min(ZN, k_lo + KR - 2) : (float)ZN;
-                in.pad0 = in.pad1 = 0;
+                in.inv_span = in.kz_hi > in.kz_lo ? 1.f / (in.kz_hi - in.kz_lo) : 0.f;
+                in.pad1 = 0;
                 s_info[b] = in;
                 mbar_arrive_expect_tx(&s_full[b], (uint32_t)(nbox * KB * CB * 4));
             }
@@ -438,16 +442,18 @@ __device__ __forceinline__ void proj_t_tile(const ProjArgs &a, const CUtensorMap
             const bool staged = in.fits && m <= 3;
             const int2 cd = make_int2(staged ? ia - in.c_lo : ia, dc);
             if (staged) {
-                // address of row k, column a = bits(k + 2^23) * RS4 + base (mod 2^32)
+                // address of row k_lo + i, column a = bits(i + 2^23) * RS4 + base (mod 2^32)
                 const uint32_t base = stage_addr + (uint32_t)b * 4u * (uint32_t)stage_floats + 4u * (uint32_t)cd.x -
-                                      (uint32_t)in.k_lo * RS4 - 0x4B000000u * RS4;
-                const float kzlo = in.kz_lo, kzhi = in.kz_hi;
+                                      0x4B000000u * RS4;
+                // kz normalised to the box: (T e + z0 - kz_lo) / span
+                const float span = in.kz_hi - in.kz_lo;
+                const float Tn = te.T * in.inv_span, z0n = (z0 - in.kz_lo) * in.inv_span;
                 if (m <= 1)
-                    rows_narrow<NR>(acc, te, dc, e_addr, base, RS4, z0, kzlo, kzhi);
+                    rows_narrow<NR>(acc, te, dc, e_addr, base, RS4, Tn, z0n, span);
                 else if (m == 2)
-                    rows_wide<NR, 2>(acc, te, dc, e_addr, base, RS4, z0, kzlo, kzhi);
+                    rows_wide<NR, 2>(acc, te, dc, e_addr, base, RS4, Tn, z0n, span);
                 else
-                    rows_wide<NR, 3>(acc, te, dc, e_addr, base, RS4, z0, kzlo, kzhi);
+                    rows_wide<NR, 3>(acc, te, dc, e_addr, base, RS4, Tn, z0n, span);
             } else {
                 // block wider than a stage, or strips wider than four columns:
                 // the column prefixes from global memory
