@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(kCols * ZS, 1) dd3_back_t_kernel(BackArgs a, i
     __shared__ __align__(16) ASet s_aset[kGeo][kCols];
 
     const int tid = threadIdx.x;
-    const int bx0 = blockIdx.x * kB, by0 = blockIdx.y * kB;
+    const int bx0 = blockIdx.x * kB, by0 = (blockIdx.y + a.by_off) * kB;
     const int col = tid & (kCols - 1), zs = tid / kCols;
     const int cx = col & (kB - 1), cy = col / kB;
     const int x = bx0 + cx, y = by0 + cy;
@@ -579,7 +579,10 @@ cudaError_t launch_k(const BackArgs &a, cudaStream_t s)
     auto kern = dd3_back_t_kernel<ZS, KSEG, VPT, ZSKIP>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    dim3 grid((a.XN + kB - 1) / kB, (a.YN + kB - 1) / kB, (a.ZN + ZS * KSEG - 1) / (ZS * KSEG));
+    const int bys = (a.YN + kB - 1) / kB;
+    if (a.by_off < 0 || a.by_count < 0 || (a.by_count == 0 && a.by_off != 0) || a.by_off + a.by_count > bys)
+        return cudaErrorInvalidValue;
+    dim3 grid((a.XN + kB - 1) / kB, a.by_count > 0 ? a.by_count : bys, (a.ZN + ZS * KSEG - 1) / (ZS * KSEG));
     if (ZSKIP && a.zrange) {
         zrange_kernel<<<grid.z, 256, 0, s>>>(a, ZS * KSEG, a.zrange);
         e = cudaGetLastError();

@@ -131,6 +131,10 @@ cudaError_t launch_volume_sat(const float *vol, const unsigned char *mask, int X
 // orientation 0: slices y, columns x (Z_y); 1: slices x, columns y (Z_x).
 cudaError_t launch_zt(const float *vol, const unsigned char *mask, int XN, int YN, int ZN, int orientation,
                       float *out, int rs, cudaStream_t s);
+// The same for the voxel columns with y in [y0, y1) only (y0 a multiple of
+// 32), so a volume uploaded in y slabs can be prefixed slab by slab.
+cudaError_t launch_zt_rows(const float *vol, const unsigned char *mask, int XN, int YN, int ZN, int orientation,
+                           float *out, int rs, int y0, int y1, cudaStream_t s);
 
 // Projection SAT: Q[p][u'][v'] of W = prj * L (L = slab path weight of the
 // view's driving axis) for n views of the list.
@@ -290,6 +294,7 @@ struct BackArgs {
     const float *pv;      // projection v-prefixes [n][DNU][vp] (sat mode ZPREFIX)
     int zskip;            // a helical scan: views may miss a CTA's z range (tested, then skipped)
     int2 *zrange;         // device scratch, one per z block: list positions [x, y) that can meet it
+    int by_off, by_count; // z-prefix mode: brick rows [by_off, by_off + by_count) only (by_count 0: all)
 };
 cudaError_t launch_back(const BackArgs &a, cudaStream_t s, int *launches);
 // Backprojector on projection v-prefixes (sat mode ZPREFIX).

@@ -6,6 +6,17 @@
 // Geometry plans and device buffers are cached per device (re-created only
 // when the geometry changes, buffers only grow), so repeated calls with one
 // scan geometry pay no allocation.  Calls on one device are serialised.
+//
+// The copies run on a second stream and overlap the compute chunk by chunk
+// (z-prefix plans): the volume goes up in y slabs, each slab's column
+// z-prefixes built as it lands; projections come back in blocks of view
+// groups as they are finished; the projections of a backprojection go up in
+// view blocks, each block's v-prefixes built as it lands, and the volume
+// comes back in y slabs of bricks as they are finished.  Every chunk runs the
+// same per-output arithmetic as the one-launch path, so the results are the
+// same bit for bit.  Pageable host buffers are staged through a pinned ring
+// (transfer.h).
+#include <climits>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -13,6 +24,7 @@
 #include <random>
 
 #include "plan.h"
+#include "transfer.h"
 
 using namespace ctlab;
 
@@ -30,7 +42,17 @@ struct LegacyCtx {
     unsigned char *d_mask = nullptr;
     size_t mask_cap = 0;
     cudaStream_t stream = nullptr;
+    Stager stager;
+    std::vector<cudaEvent_t> ev; // chunk completion events (compute and copy streams)
+    // projection chunks of the cached plan: consecutive view groups whose
+    // views are the list positions [cut[k], cut[k+1])
+    const ctlab_plan *chunk_plan = nullptr;
+    std::vector<int> cut;
+    std::vector<GroupTab> chunk_groups;
+    int *d_chunk_groups = nullptr;
 };
+
+constexpr int kChunks = 4;
 
 constexpr int kMaxDevices = 64;
 LegacyCtx g_ctx[kMaxDevices];
@@ -88,6 +110,13 @@ int legacy_prepare(LegacyCtx &c, const ctlab_geometry &g, int gpunum)
         cudaError_t e = cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking);
         if (e != cudaSuccess) return cuda_status(e, "legacy stream");
     }
+    if (int rc = c.stager.init(); rc != CTLAB_OK) return rc;
+    while (c.ev.size() < 2 * kChunks) {
+        cudaEvent_t e = nullptr;
+        cudaError_t ce = cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+        if (ce != cudaSuccess) return cuda_status(ce, "legacy event");
+        c.ev.push_back(e);
+    }
     // SAT arithmetic of the cached plan: slice-major FP64-accumulated
     // z-prefixes unless CTLAB_LEGACY_SAT selects 0 (2-D FP64 SAT) or 1
     // (compensated FP32 pairs)
@@ -100,6 +129,7 @@ int legacy_prepare(LegacyCtx &c, const ctlab_geometry &g, int gpunum)
     if (!c.plan || c.key != key || c.mode != mode) {
         if (c.plan) ctlab_plan_destroy(c.plan);
         c.plan = nullptr;
+        c.chunk_plan = nullptr; // a new plan may reuse the old one's address
         int rc = ctlab_plan_create(&g, gpunum, mode, &c.plan);
         if (rc != CTLAB_OK) return rc;
         c.key = key;
@@ -125,6 +155,202 @@ ctlab_geometry make_geom(float x0, float y0, float z0, int DNU, int DNV, float *
     g.XN = XN; g.YN = YN; g.ZN = ZN;
     g.dx = dx; g.dz = dz;
     return g;
+}
+
+// Splits the plan's projector view groups (over the whole view list) into
+// about kChunks runs of consecutive groups whose views are contiguous list
+// positions, and uploads each run's group table; one run when the groups do
+// not line up that way.  Cached per plan.
+int plan_chunks(LegacyCtx &c)
+{
+    ctlab_plan *p = c.plan;
+    if (c.chunk_plan == p) return CTLAB_OK;
+    c.chunk_plan = nullptr;
+    c.cut.clear();
+    c.chunk_groups.clear();
+    const HostGeometry &g = p->g;
+    std::vector<int> all(g.PN);
+    for (int i = 0; i < g.PN; ++i) all[i] = i;
+    ProjGroups pg = p->sat_mode == CTLAB_SAT_ZPREFIX ? proj_t_make_groups(g, all, p->tst)
+                                                     : proj_make_groups(g, all, p->proj_cmax);
+    const int G = pg.G, ng = pg.ngroups;
+    // each group's views are consecutive list positions; ordered by their
+    // first position the groups tile the list, and runs of them make chunks
+    std::vector<std::pair<int, int>> order; // (first position, group)
+    bool tiles = G >= 1 && ng >= 1;
+    for (int k = 0; k < ng && tiles; ++k) {
+        int lo = INT_MAX, hi = -1, cnt = 0;
+        for (int q = 0; q < G; ++q) {
+            const int v = pg.table[(size_t)k * G + q];
+            if (v < 0) continue;
+            lo = std::min(lo, v);
+            hi = std::max(hi, v);
+            ++cnt;
+        }
+        if (cnt == 0 || hi - lo + 1 != cnt) tiles = false;
+        order.push_back({lo, k});
+    }
+    std::vector<int> table; // the groups in position order
+    std::vector<int> gcut = {0}, pcut = {0};
+    if (tiles) {
+        std::sort(order.begin(), order.end());
+        int seen = 0;
+        for (int i = 0; i < ng && tiles; ++i) {
+            const int k = order[i].second;
+            if (order[i].first != seen) tiles = false;
+            int cnt = 0;
+            for (int q = 0; q < G; ++q) {
+                table.push_back(pg.table[(size_t)k * G + q]);
+                cnt += pg.table[(size_t)k * G + q] >= 0;
+            }
+            seen += cnt;
+            const int want = (int)pcut.size() * g.PN / kChunks;
+            if (tiles && seen >= want && i + 1 < ng && (int)pcut.size() < kChunks) {
+                gcut.push_back(i + 1);
+                pcut.push_back(seen);
+            }
+        }
+        if (seen != g.PN) tiles = false;
+    }
+    if (!tiles) { // one chunk: the table as planned
+        table = pg.table;
+        gcut = {0};
+        pcut = {0};
+    }
+    gcut.push_back(ng);
+    pcut.push_back(g.PN);
+    pg.table = table;
+    if (c.d_chunk_groups) cudaFree(c.d_chunk_groups);
+    c.d_chunk_groups = nullptr;
+    cudaError_t ce = cudaMalloc(&c.d_chunk_groups, sizeof(int) * std::max<size_t>(pg.table.size(), 1));
+    if (ce != cudaSuccess) return cuda_status(ce, "legacy chunk groups");
+    // positions in a run's table are relative to the run's first view
+    std::vector<int> tab(pg.table.size());
+    for (size_t k = 0; k + 1 < gcut.size(); ++k)
+        for (int i = gcut[k] * G; i < gcut[k + 1] * G; ++i)
+            tab[i] = pg.table[i] < 0 ? -1 : pg.table[i] - pcut[k];
+    if (!tab.empty())
+        CTLAB_CUDA_TRY(cudaMemcpy(c.d_chunk_groups, tab.data(), sizeof(int) * tab.size(), cudaMemcpyHostToDevice));
+    for (size_t k = 0; k + 1 < gcut.size(); ++k) {
+        GroupTab t;
+        t.d = c.d_chunk_groups + (size_t)gcut[k] * G;
+        t.ngroups = gcut[k + 1] - gcut[k];
+        t.G = G;
+        c.chunk_groups.push_back(t);
+    }
+    c.cut = pcut;
+    c.chunk_plan = p;
+    return CTLAB_OK;
+}
+
+// y slabs of kChunks parts (boundaries multiples of 32, for the x-slice
+// z-prefixes) -- or of 8-voxel brick rows for the backprojector
+std::vector<int> y_cuts(int YN, int align)
+{
+    std::vector<int> cut = {0};
+    for (int k = 1; k < kChunks; ++k) {
+        const int y = (int)((long long)k * YN / kChunks) / align * align;
+        if (y > cut.back() && y < YN) cut.push_back(y);
+    }
+    cut.push_back(YN);
+    return cut;
+}
+
+int legacy_proj(LegacyCtx &c, const float *hvol, float *hprj, const unsigned char *mask)
+{
+    ctlab_plan *p = c.plan;
+    const HostGeometry &g = p->g;
+    const size_t col = (size_t)g.XN * g.ZN, bin = (size_t)g.DNU * g.DNV;
+    cudaStream_t s = c.stream;
+    Stager &st = c.stager;
+    p->last_launches = 0;
+    int rc = plan_chunks(c);
+    if (rc != CTLAB_OK) return rc;
+    // mask, then the volume in y slabs; z-prefix plans build each slab's
+    // column prefixes as it lands
+    if (mask) rc = st.h2d(c.d_mask, mask, (size_t)g.XN * g.YN, nullptr);
+    const unsigned char *dm = mask ? c.d_mask : nullptr;
+    if (p->sat_mode == CTLAB_SAT_ZPREFIX) {
+        const std::vector<int> yc = y_cuts(g.YN, 32);
+        for (size_t k = 0; k + 1 < yc.size() && rc == CTLAB_OK; ++k) {
+            rc = st.h2d(c.d_vol + yc[k] * col, hvol + yc[k] * col, (yc[k + 1] - yc[k]) * col * sizeof(float), nullptr);
+            if (rc == CTLAB_OK) CTLAB_CUDA_TRY(cudaEventRecord(c.ev[k], st.stream()));
+            if (rc == CTLAB_OK) CTLAB_CUDA_TRY(cudaStreamWaitEvent(s, c.ev[k], 0));
+            if (rc == CTLAB_OK) rc = plan_volume_sat_rows(p, c.d_vol, dm, yc[k], yc[k + 1], s);
+        }
+    } else {
+        if (rc == CTLAB_OK) rc = st.h2d(c.d_vol, hvol, g.YN * col * sizeof(float), nullptr);
+        if (rc == CTLAB_OK) CTLAB_CUDA_TRY(cudaEventRecord(c.ev[0], st.stream()));
+        if (rc == CTLAB_OK) CTLAB_CUDA_TRY(cudaStreamWaitEvent(s, c.ev[0], 0));
+        if (rc == CTLAB_OK) rc = plan_volume_sat(p, c.d_vol, dm, s);
+    }
+    // projection by runs of view groups, each run's views downloaded as soon
+    // as it is done
+    for (size_t k = 0; k + 1 < c.cut.size() && rc == CTLAB_OK; ++k) {
+        const int v0 = c.cut[k], n = c.cut[k + 1] - v0;
+        rc = plan_proj_list(p, p->d_all_views + v0, n, c.chunk_groups[k], c.d_prj + bin * v0, s, PROJ_PLAIN, nullptr,
+                            nullptr, nullptr);
+        if (rc == CTLAB_OK) CTLAB_CUDA_TRY(cudaEventRecord(c.ev[kChunks + k], s));
+        if (rc == CTLAB_OK) rc = st.d2h(hprj + bin * v0, c.d_prj + bin * v0, bin * n * sizeof(float), c.ev[kChunks + k]);
+    }
+    if (rc == CTLAB_OK) rc = st.finish();
+    if (rc != CTLAB_OK) {
+        st.abandon();
+        return rc;
+    }
+    return plan_check_device_error(p, s);
+}
+
+int legacy_back(LegacyCtx &c, const float *hprj, float *hvol, const unsigned char *mask)
+{
+    ctlab_plan *p = c.plan;
+    const HostGeometry &g = p->g;
+    if (!g.flat_uniform)
+        return set_status(CTLAB_ERR_UNSUPPORTED, "backprojection needs a flat detector with uniform u and v pitch");
+    if (p->q_capacity == 0)
+        return set_status(CTLAB_ERR_UNSUPPORTED, "DNV beyond the backprojector's shared-memory tiles");
+    const size_t col = (size_t)g.XN * g.ZN, bin = (size_t)g.DNU * g.DNV;
+    cudaStream_t s = c.stream;
+    Stager &st = c.stager;
+    p->last_launches = 0;
+    int rc = CTLAB_OK;
+    if (mask) rc = st.h2d(c.d_mask, mask, (size_t)g.XN * g.YN, nullptr);
+    const unsigned char *dm = mask ? c.d_mask : nullptr;
+    if (p->sat_mode != CTLAB_SAT_ZPREFIX) {
+        if (rc == CTLAB_OK) rc = st.h2d(c.d_prj, hprj, bin * g.PN * sizeof(float), nullptr);
+        if (rc == CTLAB_OK) CTLAB_CUDA_TRY(cudaEventRecord(c.ev[0], st.stream()));
+        if (rc == CTLAB_OK) CTLAB_CUDA_TRY(cudaStreamWaitEvent(s, c.ev[0], 0));
+        if (rc == CTLAB_OK) rc = ctlab_back(p, c.d_prj, dm, c.d_vol, s);
+        if (rc == CTLAB_OK) CTLAB_CUDA_TRY(cudaEventRecord(c.ev[kChunks], s));
+        if (rc == CTLAB_OK) rc = st.d2h(hvol, c.d_vol, g.YN * col * sizeof(float), c.ev[kChunks]);
+    } else {
+        // projections in view blocks, each block's v-prefixes built as it lands
+        for (int k = 0; k < kChunks && rc == CTLAB_OK; ++k) {
+            const int v0 = (int)((long long)k * g.PN / kChunks), v1 = (int)((long long)(k + 1) * g.PN / kChunks);
+            if (v1 == v0) continue;
+            rc = st.h2d(c.d_prj + bin * v0, hprj + bin * v0, bin * (v1 - v0) * sizeof(float), nullptr);
+            if (rc == CTLAB_OK) CTLAB_CUDA_TRY(cudaEventRecord(c.ev[k], st.stream()));
+            if (rc == CTLAB_OK) CTLAB_CUDA_TRY(cudaStreamWaitEvent(s, c.ev[k], 0));
+            if (rc == CTLAB_OK) rc = plan_proj_sat_range(p, p->d_all_views, v0, v1 - v0, c.d_prj, s);
+        }
+        // the volume in y slabs of brick rows, each downloaded when done
+        const int bys = (g.YN + 7) / 8;
+        const std::vector<int> bc = y_cuts(bys, 1);
+        for (size_t k = 0; k + 1 < bc.size() && rc == CTLAB_OK; ++k) {
+            rc = plan_back_rows(p, p->d_all_views, g.PN, dm, c.d_vol, s, BACK_PLAIN, nullptr, 1.f, 0, 0.f, 0.f,
+                                bc[k], bc[k + 1] - bc[k]);
+            if (rc == CTLAB_OK) CTLAB_CUDA_TRY(cudaEventRecord(c.ev[kChunks + k], s));
+            const size_t y0 = (size_t)bc[k] * 8, y1 = std::min<size_t>((size_t)bc[k + 1] * 8, g.YN);
+            if (rc == CTLAB_OK)
+                rc = st.d2h(hvol + y0 * col, c.d_vol + y0 * col, (y1 - y0) * col * sizeof(float), c.ev[kChunks + k]);
+        }
+    }
+    if (rc == CTLAB_OK) rc = st.finish();
+    if (rc != CTLAB_OK) {
+        st.abandon();
+        return rc;
+    }
+    return plan_check_device_error(p, s);
 }
 
 int check_gpu(int gpunum)
@@ -160,21 +386,7 @@ void DD3Proj_gpu(float x0, float y0, float z0, int DNU, int DNV, float *xds, flo
     ctlab_geometry g = make_geom(x0, y0, z0, DNU, DNV, xds, yds, zds, imgXCenter, imgYCenter, imgZCenter, hangs,
                                  hzPos, PN, XN, YN, ZN, dx, dz);
     if (legacy_prepare(c, g, gpunum) != CTLAB_OK) return;
-    const size_t nv = (size_t)XN * YN * ZN, np = (size_t)PN * DNU * DNV;
-    cudaError_t e = cudaMemcpyAsync(c.d_vol, hvol, nv * sizeof(float), cudaMemcpyHostToDevice, c.stream);
-    if (e == cudaSuccess && mask)
-        e = cudaMemcpyAsync(c.d_mask, mask, (size_t)XN * YN, cudaMemcpyHostToDevice, c.stream);
-    if (e != cudaSuccess) {
-        cuda_status(e, "DD3Proj_gpu upload");
-        return;
-    }
-    if (ctlab_proj(c.plan, c.d_vol, mask ? c.d_mask : nullptr, c.d_prj, c.stream) != CTLAB_OK) return;
-    e = cudaMemcpyAsync(hprj, c.d_prj, np * sizeof(float), cudaMemcpyDeviceToHost, c.stream);
-    if (e != cudaSuccess) {
-        cuda_status(e, "DD3Proj_gpu download");
-        return;
-    }
-    if (plan_check_device_error(c.plan, c.stream) != CTLAB_OK) return;
+    if (legacy_proj(c, hvol, hprj, mask) != CTLAB_OK) return;
     ok();
 }
 
@@ -199,21 +411,7 @@ void DD3Back_gpu(float x0, float y0, float z0, int DNU, int DNV, float *xds, flo
     ctlab_geometry g = make_geom(x0, y0, z0, DNU, DNV, xds, yds, zds, imgXCenter, imgYCenter, imgZCenter, hangs,
                                  hzPos, PN, XN, YN, ZN, dx, dz);
     if (legacy_prepare(c, g, gpunum) != CTLAB_OK) return;
-    const size_t nv = (size_t)XN * YN * ZN, np = (size_t)PN * DNU * DNV;
-    cudaError_t e = cudaMemcpyAsync(c.d_prj, hprj, np * sizeof(float), cudaMemcpyHostToDevice, c.stream);
-    if (e == cudaSuccess && mask)
-        e = cudaMemcpyAsync(c.d_mask, mask, (size_t)XN * YN, cudaMemcpyHostToDevice, c.stream);
-    if (e != cudaSuccess) {
-        cuda_status(e, "DD3Back_gpu upload");
-        return;
-    }
-    if (ctlab_back(c.plan, c.d_prj, mask ? c.d_mask : nullptr, c.d_vol, c.stream) != CTLAB_OK) return;
-    e = cudaMemcpyAsync(hvol, c.d_vol, nv * sizeof(float), cudaMemcpyDeviceToHost, c.stream);
-    if (e != cudaSuccess) {
-        cuda_status(e, "DD3Back_gpu download");
-        return;
-    }
-    if (plan_check_device_error(c.plan, c.stream) != CTLAB_OK) return;
+    if (legacy_back(c, hprj, hvol, mask) != CTLAB_OK) return;
     ok();
 }
 

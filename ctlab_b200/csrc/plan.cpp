@@ -189,6 +189,48 @@ int plan_proj_list(ctlab_plan *p, const int *d_list, int n, const GroupTab &gt, 
     return CTLAB_OK;
 }
 
+int plan_volume_sat_rows(ctlab_plan *p, const float *d_vol, const unsigned char *d_mask, int y0, int y1,
+                         cudaStream_t s)
+{
+    const HostGeometry &g = p->g;
+    if (p->sat_mode != CTLAB_SAT_ZPREFIX) return set_status(CTLAB_ERR_INTERNAL, "row-range SAT needs z-prefix mode");
+    if (p->need_y) {
+        cudaError_t e = launch_zt_rows(d_vol, d_mask, g.XN, g.YN, g.ZN, 0, p->d_zt_y, p->zt_rs_y, y0, y1, s);
+        if (e != cudaSuccess) return cuda_status(e, "z-prefixes (y slices, row range)");
+        ++p->last_launches;
+    }
+    if (p->need_x) {
+        cudaError_t e = launch_zt_rows(d_vol, d_mask, g.XN, g.YN, g.ZN, 1, p->d_zt_x, p->zt_rs_x, y0, y1, s);
+        if (e != cudaSuccess) return cuda_status(e, "z-prefixes (x slices, row range)");
+        ++p->last_launches;
+    }
+    return CTLAB_OK;
+}
+
+int plan_proj_sat_range(ctlab_plan *p, const int *d_list, int first, int n, const float *d_prj, cudaStream_t s)
+{
+    const HostGeometry &g = p->g;
+    if (p->sat_mode != CTLAB_SAT_ZPREFIX) return set_status(CTLAB_ERR_INTERNAL, "view-range prefixes need z-prefix mode");
+    if (first < 0 || n < 0 || first + n > p->q_capacity)
+        return set_status(CTLAB_ERR_INTERNAL, "projection prefix capacity exceeded");
+    if (n == 0) return CTLAB_OK;
+    ProjSatArgs a;
+    a.prj = d_prj + (size_t)first * g.DNU * g.DNV;
+    a.views = p->d_views;
+    a.view_list = d_list + first;
+    a.n = n;
+    a.det = p->d_det;
+    a.DNU = g.DNU; a.DNV = g.DNV;
+    a.dx = g.dx;
+    a.out = p->d_q;
+    a.vp = p->vp;
+    a.f32pair = 0;
+    cudaError_t e = launch_pv(a, p->d_pv + (size_t)first * g.DNU * p->vp, p->vp, s);
+    if (e != cudaSuccess) return cuda_status(e, "projection v-prefixes (view range)");
+    ++p->last_launches;
+    return CTLAB_OK;
+}
+
 int plan_proj_sat(ctlab_plan *p, const int *d_list, int n, const float *d_prj, cudaStream_t s)
 {
     const HostGeometry &g = p->g;
@@ -221,6 +263,15 @@ int plan_back_list(ctlab_plan *p, const int *d_list, int n, const unsigned char 
                    cudaStream_t s, int epilogue, const float *col_sum, float lambda, int clamp, float min_v,
                    float max_v)
 {
+    return plan_back_rows(p, d_list, n, d_mask, d_vol, s, epilogue, col_sum, lambda, clamp, min_v, max_v, 0, 0);
+}
+
+int plan_back_rows(ctlab_plan *p, const int *d_list, int n, const unsigned char *d_mask, float *d_vol,
+                   cudaStream_t s, int epilogue, const float *col_sum, float lambda, int clamp, float min_v,
+                   float max_v, int by_off, int by_count)
+{
+    if ((by_off != 0 || by_count != 0) && (p->sat_mode != CTLAB_SAT_ZPREFIX || n == 0))
+        return set_status(CTLAB_ERR_INTERNAL, "brick-row ranges need z-prefix mode and views");
     const HostGeometry &g = p->g;
     BackArgs a;
     std::memset(&a, 0, sizeof a);
@@ -250,6 +301,8 @@ int plan_back_list(ctlab_plan *p, const int *d_list, int n, const unsigned char 
     a.err = p->d_err;
     a.pv = p->d_pv;
     a.zrange = p->d_zrange;
+    a.by_off = by_off;
+    a.by_count = by_count;
     for (const DevView &V : g.views)
         if (V.zP != g.views[0].zP) a.zskip = 1; // a helical scan
     if (n == 0 && epilogue == BACK_PLAIN) {

@@ -73,6 +73,16 @@ int plan_back_list(ctlab_plan *p, const int *d_list, int n, const unsigned char 
                    cudaStream_t s, int epilogue, const float *col_sum, float lambda, int clamp, float min_v,
                    float max_v);
 int plan_upload_list(ctlab_plan *p, const int *h_views, int n, cudaStream_t s);
+// z-prefix plans only, for copies overlapped with compute: the volume's
+// z-prefixes of the voxel columns with y in [y0, y1) (y0 a multiple of 32);
+// the projection v-prefixes of list positions [first, first + n); the
+// backprojection of brick rows [by_off, by_off + by_count) (8 voxel rows each).
+int plan_volume_sat_rows(ctlab_plan *p, const float *d_vol, const unsigned char *d_mask, int y0, int y1,
+                         cudaStream_t s);
+int plan_proj_sat_range(ctlab_plan *p, const int *d_list, int first, int n, const float *d_prj, cudaStream_t s);
+int plan_back_rows(ctlab_plan *p, const int *d_list, int n, const unsigned char *d_mask, float *d_vol,
+                   cudaStream_t s, int epilogue, const float *col_sum, float lambda, int clamp, float min_v,
+                   float max_v, int by_off, int by_count);
 int plan_check_device_error(ctlab_plan *p, cudaStream_t s);
 void timing_mark(ctlab_plan *p, int which, cudaStream_t s);
 // TMA map of the plan's z-prefix array of one orientation for a staging.

@@ -321,11 +321,12 @@ namespace {
 // scan plus a carried FP64 total), the rounded prefixes go through a padded
 // shared tile, and the CTA writes them out as rows of 32 adjacent columns.
 __global__ void __launch_bounds__(256) zt_kernel(const float *__restrict__ vol, const unsigned char *mask, int XN,
-                                                 int ZN, int nb, int orientation, float *__restrict__ out, int rs)
+                                                 int ZN, int nb, int orientation, float *__restrict__ out, int rs,
+                                                 int j0, int c_off)
 {
     __shared__ float tile[32][33];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int j = blockIdx.y, c0 = blockIdx.x * 32;
+    const int j = blockIdx.y + j0, c0 = blockIdx.x * 32 + c_off;
     const float *col[4];
     float m[4];
     double carry[4];
@@ -370,10 +371,27 @@ __global__ void __launch_bounds__(256) zt_kernel(const float *__restrict__ vol, 
 cudaError_t launch_zt(const float *vol, const unsigned char *mask, int XN, int YN, int ZN, int orientation,
                       float *out, int rs, cudaStream_t s)
 {
+    return launch_zt_rows(vol, mask, XN, YN, ZN, orientation, out, rs, 0, YN, s);
+}
+
+cudaError_t launch_zt_rows(const float *vol, const unsigned char *mask, int XN, int YN, int ZN, int orientation,
+                           float *out, int rs, int y0, int y1, cudaStream_t s)
+{
     const int nb = orientation ? YN : XN, na = orientation ? XN : YN;
-    if (rs < nb || na > 65535) return cudaErrorInvalidValue;
-    dim3 grid((rs + 31) / 32, na);
-    zt_kernel<<<grid, 256, 0, s>>>(vol, mask, XN, ZN, nb, orientation, out, rs);
+    if (rs < nb || na > 65535 || y0 < 0 || y1 > YN || y0 > y1) return cudaErrorInvalidValue;
+    if (y1 == y0) return cudaSuccess;
+    if (orientation == 0) {
+        // slices y0 .. y1-1, every column
+        dim3 grid((rs + 31) / 32, y1 - y0);
+        zt_kernel<<<grid, 256, 0, s>>>(vol, mask, XN, ZN, nb, 0, out, rs, y0, 0);
+    } else {
+        // every slice, columns y0 .. y1-1 (y0 a multiple of 32; the range that
+        // ends the volume also covers the pad columns up to rs)
+        if (y0 % 32) return cudaErrorInvalidValue;
+        const int c1 = y1 == YN ? rs : y1;
+        dim3 grid((c1 - y0 + 31) / 32, na);
+        zt_kernel<<<grid, 256, 0, s>>>(vol, mask, XN, ZN, nb, 1, out, rs, 0, y0);
+    }
     return cudaGetLastError();
 }
 

@@ -376,3 +376,37 @@ def test_zprefix_tall_volume_matches_oracle(torch_cuda, zpos):
     record_error(f"proj/tall_z_{zpos}/zprefix", ep)
     record_error(f"back/tall_z_{zpos}/zprefix", eb)
     assert ep <= REL_L2 and eb <= REL_L2, (ep, eb)
+
+
+@pytest.mark.parametrize("sat_mode", [cb.CTLAB_SAT_ZPREFIX, cb.CTLAB_SAT_FP64])
+@pytest.mark.parametrize("pinned", [False, True])
+def test_legacy_overlapped_copies_equal_plan_path(torch_cuda, sat_mode, pinned, monkeypatch):
+    """DD3Proj_gpu / DD3Back_gpu copy in chunks overlapped with the compute (the volume
+    in y slabs, the projections in blocks of view groups, the backprojection in slabs of
+    brick rows) from pinned or pageable host buffers: still bit for bit the plan path's
+    results, on a scan large enough to split (config 1, 128x128x64, 360 views)."""
+    torch = torch_cuda
+    monkeypatch.setenv("CTLAB_LEGACY_SAT", str(sat_mode))
+    g = G.config1()
+    vol = phantom(g, 9)
+    mask = (np.random.default_rng(6).random(g.XN * g.YN) > 0.2).astype(np.uint8)
+
+    def host(shape):
+        if pinned:
+            return torch.zeros(shape, dtype=torch.float32, pin_memory=True).numpy()
+        return np.zeros(shape, np.float32)
+
+    hv = host(g.vol_shape)
+    hv[...] = vol
+    hp = host(g.prj_shape)
+    cb.DD3Proj_gpu(**g.args(), hvol=hv, hprj=hp, mask=mask, gpunum=0, prjMode=0)
+    hb = host(g.vol_shape)
+    cb.DD3Back_gpu(**g.args(), hvol=hb, hprj=hp, mask=mask, gpunum=0, squared=0, prjMode=0)
+    with cb.Plan(g, sat_mode=sat_mode) as plan:
+        out = torch.zeros(g.prj_shape, dtype=torch.float32, device="cuda")
+        plan.proj(dev(torch, vol), out, mask=dev(torch, mask))
+        vb = torch.zeros(g.vol_shape, dtype=torch.float32, device="cuda")
+        plan.back(dev(torch, hp), vb, mask=dev(torch, mask))
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(out.cpu().numpy(), hp)
+        np.testing.assert_array_equal(vb.cpu().numpy(), hb)
