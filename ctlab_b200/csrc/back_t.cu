@@ -47,8 +47,8 @@ namespace {
 constexpr int kB = 8;                 // brick edge (voxel columns)
 constexpr int kCols = kB * kB;        // 64 columns per CTA
 // z segments per column ZS (template parameter): 8 (512 threads, KSEG up to
-// 32 accumulators a thread) or 16 (1024 threads, twice the warps to hide the
-// shared-memory latency of phase B, at most 64 registers a thread)
+// 32 accumulators a thread; the default) or 16 (1024 threads, twice the warps
+// to hide the shared-memory latency of phase B, at most 64 registers a thread)
 constexpr size_t kSmemPerCta = 200 * 1024; // one CTA per SM
 constexpr size_t kStaticSmem = 20 * 1024;
 constexpr int kGeo = 4;               // geometry slots (views l .. l+3)
@@ -499,13 +499,17 @@ int e_pitch(int DNV, int zs) { return (zs * vpt_of(DNV, zs)) | 1; }
 // the largest (E, dE) pitch over the two block shapes
 int e_pitch_max(int DNV) { return std::max(e_pitch(DNV, 8), e_pitch(DNV, 16)); }
 
-// z segments per column: 16 (1024 threads) unless CTLAB_BACKT_ZS=8 selects
-// the 512-thread shape; both give the same results.
+// z segments per column: 8 (512 threads), unless CTLAB_BACKT_ZS=16 selects
+// the 1024-thread shape.  Both give the same results; on the B200 the
+// 1024-thread shape is slower at 512x512x256 / 984 views (63.0 vs 57.7 ms):
+// its warps cover half the voxels each, so the per-view bookkeeping (loop,
+// waits, slot addresses) costs twice as much per voxel-view, and twice the
+// warps per barrier outweigh the latency they hide.
 int back_t_zs()
 {
     static const int zs = [] {
         const char *e = std::getenv("CTLAB_BACKT_ZS");
-        return (e && std::atoi(e) == 8) ? 8 : 16;
+        return (e && std::atoi(e) == 16) ? 16 : 8;
     }();
     return zs;
 }
