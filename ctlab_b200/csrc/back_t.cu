@@ -130,12 +130,16 @@ __device__ __forceinline__ double u_of(const DevView &V, double px, double py)
 }
 
 template <int ZS, int KSEG, int VPT, bool ZSKIP>
-__global__ void __launch_bounds__(kCols * ZS, 1) dd3_back_t_kernel(BackArgs a, int es2, int rmax)
+__global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel(BackArgs a, int es2, int rmax)
 {
     extern __shared__ __align__(128) unsigned char smem[];
     const int vp = a.vp; // P row pitch (floats, multiple of 4)
-    float2 *E2 = reinterpret_cast<float2 *>(smem);                      // [2][kCols][es2] (E, dE)
-    float *pbuf = reinterpret_cast<float *>(E2 + 2 * (size_t)kCols * es2); // [2][rmax][vp]
+    // (E, dE) tables: double buffered (B of a view overlaps A of the next) in
+    // the 512- and 1024-thread shapes, single buffered in the 256-thread one,
+    // which runs two CTAs per SM and separates B from the next A by a barrier
+    constexpr int EB = ZS == 4 ? 1 : 2;
+    float2 *E2 = reinterpret_cast<float2 *>(smem);                       // [EB][kCols][es2] (E, dE)
+    float *pbuf = reinterpret_cast<float *>(E2 + EB * (size_t)kCols * es2); // [2][rmax][vp]
     __shared__ __align__(8) uint64_t s_bar[2];
     __shared__ int s_ulo[2], s_rows[2];
     __shared__ double s_u[kGeo][kB][kB + 1];
@@ -240,11 +244,12 @@ __global__ void __launch_bounds__(kCols * ZS, 1) dd3_back_t_kernel(BackArgs a, i
     };
 
     // phase-A set-up of list entry l into slot l % kGeo (threads 256..319,
-    // one per column): the same staging origin as issue(l), from the same
+    // or 192..255 in the 256-thread shape; one per column): the same staging origin as issue(l), from the same
     // corner boundaries
     auto setup = [&](int l) {
-        if (l >= n || tid < 256 || tid >= 256 + kCols) return;
-        const int c = tid - 256, sl = l % kGeo;
+        constexpr int kSet0 = ZS == 4 ? 192 : 256; // a pair of warps the geometry leaves free
+        if (l >= n || tid < kSet0 || tid >= kSet0 + kCols) return;
+        const int c = tid - kSet0, sl = l % kGeo;
         const int ccx = c & (kB - 1), ccy = c / kB;
         const double u0 = s_u[sl][0][0], u1 = s_u[sl][0][kB], u2 = s_u[sl][kB - 1][0], u3 = s_u[sl][kB - 1][kB];
         const double umin = fmin(fmax(fmin(fmin(u0, u1), fmin(u2, u3)), 0.0), (double)(DNU - 1));
@@ -316,7 +321,8 @@ __global__ void __launch_bounds__(kCols * ZS, 1) dd3_back_t_kernel(BackArgs a, i
         // warp-uniform, so the warp collectives of phase A stay converged
         if (__any_sync(0xffffffffu, !mbar_wait(&s_bar[b], (uint32_t)((li >> 1) & 1)))) timed_out = true;
         const int xdrv = s_xdrv[ls];
-        float2 *E = E2 + (size_t)b * kCols * es2; // double buffered: B(li) overlaps A(li+1)
+        const int eb = EB == 2 ? b : 0;
+        float2 *E = E2 + (size_t)eb * kCols * es2; // double buffered: B(li) overlaps A(li+1)
 
         // ---- A: (E_c(i), E_c(i+1) - E_c(i)) for i in [0, DNV], E_c(DNV+1) = E_c(DNV) ----
         // the thread's column strip for this view, recomputed from s_u (the
@@ -369,7 +375,7 @@ __global__ void __launch_bounds__(kCols * ZS, 1) dd3_back_t_kernel(BackArgs a, i
             const float wmv[3] = {__uint_as_float(q1.w), __uint_as_float(q2.x), __uint_as_float(q2.y)};
             // the warp runs its widest column's whole-cell count, the others with weight 0
             const int nmax = (int)__reduce_max_sync(0xffffffffu, q2.z);
-            const uint32_t eout = E2_addr + 8u * (uint32_t)((b * kCols + ac) * es2 + i0);
+            const uint32_t eout = E2_addr + 8u * (uint32_t)((eb * kCols + ac) * es2 + i0);
             switch (nmax) {
             case 0: phase_a_run<VPT, 0>(pa, pb, pm, wmv, wa, wb, eout); break;
             case 1: phase_a_run<VPT, 1>(pa, pb, pm, wmv, wa, wb, eout); break;
@@ -420,7 +426,7 @@ __global__ void __launch_bounds__(kCols * ZS, 1) dd3_back_t_kernel(BackArgs a, i
         if (in_vol && !timed_out && (!ZSKIP || rows >= 0)) {
             const float V0 = s_V0[ls][col], V1 = s_V1[ls][col];
             // address of (E, dE)_c[i] = bits(i + 2^23) * 8 + base (mod 2^32)
-            const uint32_t base = E2_addr + 8u * (uint32_t)(b * kCols * es2 + col * es2) - 8u * 0x4B000000u;
+            const uint32_t base = E2_addr + 8u * (uint32_t)(eb * kCols * es2 + col * es2) - 8u * 0x4B000000u;
             const float vb0 = fmaf(V1, (float)k0, V0);
             float prev = 0.f;
 #pragma unroll
@@ -434,6 +440,7 @@ __global__ void __launch_bounds__(kCols * ZS, 1) dd3_back_t_kernel(BackArgs a, i
                 prev = ev;
             }
         }
+        if constexpr (EB == 1) __syncthreads(); // the single E table is rewritten by the next A
     }
     if (timed_out && a.err) atomicExch(a.err, CTLAB_ERR_TIMEOUT);
 
@@ -497,7 +504,7 @@ int vpt_of(int DNV, int zs)
 }
 int e_pitch(int DNV, int zs) { return (zs * vpt_of(DNV, zs)) | 1; }
 // the largest (E, dE) pitch over the two block shapes
-int e_pitch_max(int DNV) { return std::max(e_pitch(DNV, 8), e_pitch(DNV, 16)); }
+int e_pitch_max(int DNV) { return std::max(std::max(e_pitch(DNV, 8), e_pitch(DNV, 16)), e_pitch(DNV, 4)); }
 
 // z segments per column: 8 (512 threads), unless CTLAB_BACKT_ZS=16 selects
 // the 1024-thread shape.  Both give the same results; on the B200 the
@@ -509,14 +516,15 @@ int back_t_zs()
 {
     static const int zs = [] {
         const char *e = std::getenv("CTLAB_BACKT_ZS");
-        return (e && std::atoi(e) == 16) ? 16 : 8;
+        const int v = e ? std::atoi(e) : 8;
+        return (v == 4 || v == 16) ? v : 8;
     }();
     return zs;
 }
 
-size_t dyn_smem(int rmax, int vp, int es2)
+size_t dyn_smem(int rmax, int vp, int es2, int ebuf = 2)
 {
-    return 4 * 2 * (size_t)rmax * vp + sizeof(float2) * 2 * (size_t)kCols * es2;
+    return 4 * 2 * (size_t)rmax * vp + sizeof(float2) * (size_t)ebuf * kCols * es2;
 }
 
 // Per z block of zblk voxels (one CTA each): the first and one-past-last list
@@ -579,7 +587,7 @@ template <int ZS, int KSEG, int VPT, bool ZSKIP>
 cudaError_t launch_k(const BackArgs &a, cudaStream_t s)
 {
     const int es2 = e_pitch(a.DNV, ZS); // (E, dE) pairs per column, odd pitch
-    const size_t sm = dyn_smem(a.rmax, a.vp, es2);
+    const size_t sm = dyn_smem(a.rmax, a.vp, es2, ZS == 4 ? 1 : 2);
     auto kern = dd3_back_t_kernel<ZS, KSEG, VPT, ZSKIP>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
@@ -598,8 +606,8 @@ cudaError_t launch_k(const BackArgs &a, cudaStream_t s)
 
 // Segment length by ZN (z blocks of 256 voxels at most); volumes of several
 // z blocks (and helical scans) test each view against each CTA's z range and
-// skip the views whose cone misses it.  512 threads: segments up to 32
-// voxels; 1024 threads: up to 16.
+// skip the views whose cone misses it.  256 threads: segments up to 64
+// voxels; 512 threads: up to 32; 1024 threads: up to 16.
 template <int ZS, int VPT>
 cudaError_t launch_z(const BackArgs &a, cudaStream_t s)
 {
@@ -607,6 +615,7 @@ cudaError_t launch_z(const BackArgs &a, cudaStream_t s)
     if (a.ZN <= ZS * 4) return launch_k<ZS, 4, VPT, false>(a, s);
     if (a.ZN <= ZS * 8) return launch_k<ZS, 8, VPT, false>(a, s);
     if (ZS * 16 < 256 && a.ZN <= ZS * 16) return launch_k<ZS, 16, VPT, false>(a, s);
+    if (ZS * 32 < 256 && a.ZN <= ZS * 32) return launch_k<ZS, 32, VPT, false>(a, s);
     if (a.zskip || a.ZN > 256) return launch_k<ZS, KMAX, VPT, true>(a, s);
     return launch_k<ZS, KMAX, VPT, false>(a, s);
 }
@@ -636,7 +645,8 @@ bool back_t_supported(int DNV)
 // phase-A run reads (kAPh * VPT), rounded to 16 bytes
 int back_t_pitch(int DNV)
 {
-    return (std::max(DNV + 2, std::max(8 * vpt_of(DNV, 8), 16 * vpt_of(DNV, 16)) + 1) + 3) & ~3;
+    return (std::max(DNV + 2, std::max(std::max(8 * vpt_of(DNV, 8), 16 * vpt_of(DNV, 16)), 4 * vpt_of(DNV, 4)) + 1) +
+            3) & ~3;
 }
 
 // Staged P rows: the widest u footprint of any brick on the volume's outer
@@ -697,7 +707,9 @@ cudaError_t launch_back_t(const BackArgs &a, cudaStream_t s, int *launches)
 {
     if (launches) ++*launches;
     if (a.n <= 0) return cudaSuccess;
-    return back_t_zs() == 8 ? launch_vpt<8>(a, s) : launch_vpt<16>(a, s);
+    const int zs = back_t_zs();
+    if (zs == 4 && vpt_of(a.DNV, 4) != 0) return launch_vpt<4>(a, s);
+    return zs == 16 ? launch_vpt<16>(a, s) : launch_vpt<8>(a, s);
 }
 
 } // namespace ctlab
