@@ -5,8 +5,9 @@
 // accumulated in FP64 and stored in FP32 (the column differences of the 2-D
 // SAT, which the FP64 path also rounds to FP32 before use).
 //
-// One CTA (512 threads) owns an 8 x 8 brick of voxel columns and a z range of
-// 8*KSEG voxels and loops over the views.  Per view:
+// One CTA owns an 8 x 8 brick of voxel columns and a z range of ZS*KSEG
+// voxels (ZS z segments per column, one thread each: 256 threads by default,
+// two CTAs per SM) and loops over the views.  Per view:
 //   geometry   the brick's voxel boundaries across the view's driving axis
 //              (8 rows of 9 points) mapped through the source onto the flat
 //              detector (FP64); each column's centre ray gives the affine
@@ -18,17 +19,20 @@
 //              between the column's two u boundaries,
 //                 E_c(v') = sg * [ sum of P over whole cells + f_b P_b - f_a P_a ],
 //              sg orienting it like the voxel's z axis (FP32), stored with its
-//              forward difference as (E, dE) pairs; 8 threads per column each
-//              run a contiguous stretch of rows with a warp-uniform trip count;
+//              forward difference as (E, dE) pairs; ZS threads per column
+//              each run a contiguous stretch of rows with a warp-uniform trip
+//              count, from a strip set-up computed two views ahead;
 //   phase B    each voxel boundary k samples E_c linearly at
 //              v = DNV * sat(V0 + V1 k) with one 64-bit shared load and the
 //              voxel accumulates E_c(v_{k+1}) - E_c(v_k): one saturating FMA
 //              clamps, the round-toward-zero FMA with 2^23 gives floor(v)
 //              biased for the shared-memory address -- no float/int
 //              conversions.
-// E is double buffered, so one barrier per view separates A(l) from B(l) and
-// the issue of view l+2's copy.  Views whose footprint exceeds a stage read P
-// from global memory.  Epilogue: in-plane mask and optionally the OS-SART
+// In the 512- and 1024-thread shapes E is double buffered, so one barrier per
+// view separates A(l) from B(l) and the issue of view l+2's copy; the
+// 256-thread shape keeps one E table and a second barrier after B(l), the
+// other CTA on the SM filling the gaps.  Views whose footprint exceeds a
+// stage read P from global memory.  Epilogue: in-plane mask and optionally the OS-SART
 // update x = (x + lambda * acc/colSum) * mask.
 #include <algorithm>
 #include <climits>
@@ -46,9 +50,10 @@ namespace {
 
 constexpr int kB = 8;                 // brick edge (voxel columns)
 constexpr int kCols = kB * kB;        // 64 columns per CTA
-// z segments per column ZS (template parameter): 8 (512 threads, KSEG up to
-// 32 accumulators a thread; the default) or 16 (1024 threads, twice the warps
-// to hide the shared-memory latency of phase B, at most 64 registers a thread)
+// z segments per column ZS (template parameter): 4 (256 threads, KSEG up to
+// 64 accumulators a thread, single-buffered E, two CTAs per SM; the default),
+// 8 (512 threads, KSEG up to 32) or 16 (1024 threads, at most 64 registers a
+// thread)
 constexpr size_t kSmemPerCta = 200 * 1024; // one CTA per SM
 constexpr size_t kStaticSmem = 20 * 1024;
 constexpr int kGeo = 4;               // geometry slots (views l .. l+3)
@@ -506,18 +511,19 @@ int e_pitch(int DNV, int zs) { return (zs * vpt_of(DNV, zs)) | 1; }
 // the largest (E, dE) pitch over the two block shapes
 int e_pitch_max(int DNV) { return std::max(std::max(e_pitch(DNV, 8), e_pitch(DNV, 16)), e_pitch(DNV, 4)); }
 
-// z segments per column: 8 (512 threads), unless CTLAB_BACKT_ZS=16 selects
-// the 1024-thread shape.  Both give the same results; on the B200 the
-// 1024-thread shape is slower at 512x512x256 / 984 views (63.0 vs 57.7 ms):
-// its warps cover half the voxels each, so the per-view bookkeeping (loop,
-// waits, slot addresses) costs twice as much per voxel-view, and twice the
-// warps per barrier outweigh the latency they hide.
+// z segments per column: 4 (256 threads, two CTAs per SM), unless
+// CTLAB_BACKT_ZS=8 or 16 selects the 512- or 1024-thread shape.  All give
+// the same results.  On the B200 at 512x512x256 / 984 views: 52.1 ms (4),
+// 57.7 ms (8), 63.0 ms (16).  A warp's per-view bookkeeping (loop, waits,
+// slot addresses, phase-A set-up loads) is spread over the voxels of its
+// threads' segments, 64 / 32 / 16 of them; the 256-thread shape still runs
+// 16 warps per SM, as two independent CTAs whose barriers do not align.
 int back_t_zs()
 {
     static const int zs = [] {
         const char *e = std::getenv("CTLAB_BACKT_ZS");
-        const int v = e ? std::atoi(e) : 8;
-        return (v == 4 || v == 16) ? v : 8;
+        const int v = e ? std::atoi(e) : 4;
+        return (v == 8 || v == 16) ? v : 4;
     }();
     return zs;
 }
