@@ -127,7 +127,7 @@ unsigned long long scan_key(const HostGeometry &g)
 
 std::mutex g_cache_mu;
 
-bool cache_lookup(const char *path, unsigned long long key, int &gcap, int &nstage, int &zs)
+bool cache_lookup(const char *path, unsigned long long key, int &gcap, int &nstage, int &zs, int &warps)
 {
     if (!path) return false;
     std::lock_guard<std::mutex> lk(g_cache_mu);
@@ -146,20 +146,24 @@ bool cache_lookup(const char *path, unsigned long long key, int &gcap, int &nsta
             zs = 0;
             const size_t pz = line.find("\"zs\":");
             if (pz != std::string::npos && std::sscanf(line.c_str() + pz + 5, "%d", &a) == 1) zs = a;
+            warps = 15;
+            const size_t pw = line.find("\"warps\":");
+            if (pw != std::string::npos && std::sscanf(line.c_str() + pw + 8, "%d", &a) == 1) warps = a;
             return true;
         }
     }
     return false;
 }
 
-void cache_store(const char *path, unsigned long long key, int gcap, int nstage, int zs, float ms)
+void cache_store(const char *path, unsigned long long key, int gcap, int nstage, int zs, int warps, float ms)
 {
     if (!path) return;
     std::lock_guard<std::mutex> lk(g_cache_mu);
     std::ofstream f(path, std::ios::app);
-    char buf[192];
-    std::snprintf(buf, sizeof buf, "{\"scan\": \"%016llx\", \"gcap\": %d, \"nstage\": %d, \"zs\": %d, \"ms\": %.4f}\n",
-                  key, gcap, nstage, zs, ms);
+    char buf[224];
+    std::snprintf(buf, sizeof buf,
+                  "{\"scan\": \"%016llx\", \"gcap\": %d, \"nstage\": %d, \"zs\": %d, \"warps\": %d, \"ms\": %.4f}\n",
+                  key, gcap, nstage, zs, warps, ms);
     f << buf;
 }
 
@@ -198,9 +202,9 @@ int ctlab_plan_autotune(ctlab_plan *plan, const float *d_vol, float *d_prj, cons
     DeviceGuard dg(plan->device);
     const HostGeometry &g = plan->g;
     const unsigned long long key = scan_key(g);
-    int gcap = 0, ns = 0, zs = 0;
-    if (cache_lookup(cache_path, key, gcap, ns, zs)) {
-        ProjTStaging st = proj_t_staging(g, gcap, ns, zs);
+    int gcap = 0, ns = 0, zs = 0, ws = 15;
+    if (cache_lookup(cache_path, key, gcap, ns, zs, ws)) {
+        ProjTStaging st = proj_t_staging(g, gcap, ns, zs, ws);
         if (st.ok) {
             int rc = apply_staging(plan, st);
             if (rc != CTLAB_OK) return rc;
@@ -213,17 +217,18 @@ int ctlab_plan_autotune(ctlab_plan *plan, const float *d_vol, float *d_prj, cons
     CTLAB_CUDA_TRY(cudaEventCreate(&e1));
     float best = 1e30f;
     ProjTStaging best_st = plan->tst;
-    int best_g = 16, best_n = 0, best_z = 0;
+    int best_g = 16, best_n = 0, best_z = 0, best_w = 15;
     std::vector<std::vector<int>> seen;
-    // candidates: views per CTA capped at 16 / 8 / 4 / 2, detector rows split
-    // over 1 / 2 / 4 CTAs (the deepest stage ring that fits); each distinct
-    // staging timed once
+    // candidates: CTAs of 16 warps (one per SM) or of 8 warps (two per SM),
+    // views per CTA capped at 16 / 8 / 4 / 2, detector rows split over 1 / 2 /
+    // 4 CTAs (the deepest stage ring that fits); each distinct staging timed once
+    for (int w : {15, 7})
     for (int gc : {16, 8, 4, 2})
         for (int z : {1, 2, 4}) {
-            ProjTStaging st = proj_t_staging(g, gc, 0, z);
+            ProjTStaging st = proj_t_staging(g, gc, 0, z, w);
             const int n = st.nstage;
             if (!st.ok) continue;
-            const std::vector<int> sig{st.G, st.NR, st.RB, st.ZS, st.CB, st.KB, st.nstage};
+            const std::vector<int> sig{st.G, st.NR, st.RB, st.ZS, st.CB, st.KB, st.nstage, st.W};
             if (std::find(seen.begin(), seen.end(), sig) != seen.end()) continue;
             seen.push_back(sig);
             int rc = apply_staging(plan, st);
@@ -244,13 +249,14 @@ int ctlab_plan_autotune(ctlab_plan *plan, const float *d_vol, float *d_prj, cons
                 best_g = gc;
                 best_n = n;
                 best_z = z;
+                best_w = w;
             }
         }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     int rc = apply_staging(plan, best_st);
     if (rc != CTLAB_OK) return rc;
-    cache_store(cache_path, key, best_g, best_n, best_z, best);
+    cache_store(cache_path, key, best_g, best_n, best_z, best_w, best);
     if (best_ms) *best_ms = best;
     return set_status(CTLAB_OK, "");
 }

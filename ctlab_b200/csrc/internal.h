@@ -235,13 +235,16 @@ ProjStaging proj_staging(const HostGeometry &g, int zp, int elem_bytes);
 // detector z boundaries.
 struct ProjTStaging {
     int G = 1, NR = 4, RB = 1, ZS = 1, CB = 0, KB = 0, KR = 0, nstage = 2, EP = 8;
+    int W = 15; // consumer warps per CTA at most (7: two CTAs share an SM)
     size_t smem = 0;
     bool ok = false;
 };
 // gcap limits the views per CTA (launches whose views group one by one use
 // a staging planned with gcap = 1); nstage > 0 fixes the stage depth, zs > 0
-// the split of the detector rows over CTAs (1, 2 or 4).
-ProjTStaging proj_t_staging(const HostGeometry &g, int gcap = 16, int nstage = 0, int zs = 0);
+// the split of the detector rows over CTAs (1, 2 or 4); wcap the consumer
+// warps per CTA (15: one CTA of 16 warps per SM; 7: CTAs of 8 warps and at
+// most half the SM's shared memory, two per SM).
+ProjTStaging proj_t_staging(const HostGeometry &g, int gcap = 16, int nstage = 0, int zs = 0, int wcap = 0);
 size_t proj_t_smem_bytes(const ProjTStaging &st);
 
 // One scan of a batched (persistent) projector launch: its arguments and TMA

@@ -769,14 +769,18 @@ cudaError_t launch_proj_t_batch(int nr, const ProjBatchParams &cases, const int4
     }
 }
 
-ProjTStaging proj_t_staging(const HostGeometry &g, int gcap, int nstage_fix, int zs_fix)
+ProjTStaging proj_t_staging(const HostGeometry &g, int gcap, int nstage_fix, int zs_fix, int wcap)
 {
     ProjTStaging st;
     st.ok = false;
+    // consumer warps per CTA: 15 (one CTA per SM) or 7 (two CTAs per SM, each
+    // within half the shared memory); CTLAB_PROJT_WARPS picks the default
+    const int W = (wcap > 0 ? wcap : env_int("CTLAB_PROJT_WARPS", kTMaxCWarps)) <= 7 ? 7 : kTMaxCWarps;
+    const size_t smem_cap = W == kTMaxCWarps ? kTSmemLimit : kTSmemLimit / 2 - 1024;
     // CTLAB_PROJT_GMAX caps the views per CTA (1..15), CTLAB_PROJT_ZS fixes
     // the row split (1, 2, 4), CTLAB_PROJT_NSTAGE the stage depth (2..4),
     // CTLAB_PROJT_CBMAX caps the staged columns
-    const int gmax = std::max(1, std::min(std::min(env_int("CTLAB_PROJT_GMAX", kTMaxCWarps), kTMaxG), gcap));
+    const int gmax = std::max(1, std::min(std::min(env_int("CTLAB_PROJT_GMAX", W), kTMaxG), std::min(gcap, W)));
     const int want_zs = zs_fix > 0 ? zs_fix : env_int("CTLAB_PROJT_ZS", 0);
     const int want_stage = nstage_fix > 0 ? nstage_fix : env_int("CTLAB_PROJT_NSTAGE", 0);
     const int cbmax = std::min(env_int("CTLAB_PROJT_CBMAX", 256), 256);
@@ -804,10 +808,10 @@ ProjTStaging proj_t_staging(const HostGeometry &g, int gcap, int nstage_fix, int
             // keeps >= 8 rows, at least enough for <= 32 rows per warp; rows
             // per warp: the rows split evenly, rounded up to 4
             const int rb_min = (rows + 31) / 32;
-            const int RB = std::max(rb_min, std::min(kTMaxCWarps / G, (rows + 7) / 8));
-            if (RB * G > kTMaxCWarps) continue;
+            const int RB = std::max(rb_min, std::min(W / G, (rows + 7) / 8));
+            if (RB * G > W) continue;
             const int NR = std::min(32, ((rows + RB - 1) / RB + 3) & ~3);
-            const int key = (RB * G >= 12 ? 1000 : 0) + G * 10 + (4 - ZS);
+            const int key = (RB * G >= (W == kTMaxCWarps ? 12 : 6) ? 1000 : 0) + G * 10 + (4 - ZS);
             if (key <= best_key) continue;
             const int zs = (g.DNV + RB * NR - 1) / (RB * NR); // CTAs over the rows (no empty one)
             // z rows a CTA stages per slice: the clamped kz range of its
@@ -830,8 +834,9 @@ ProjTStaging proj_t_staging(const HostGeometry &g, int gcap, int nstage_fix, int
                 c.KR = nbox * KB;
                 c.nstage = ns;
                 c.EP = RB * NR + 4;
+                c.W = W;
                 c.smem = smem_bytes(c);
-                if (c.smem + kTStatic > kTSmemLimit) continue;
+                if (c.smem + kTStatic > smem_cap) continue;
                 c.ok = true;
                 best = c;
                 best_key = key;
@@ -883,7 +888,7 @@ void proj_t_split(const ProjTStaging &st, int G, int &nr, int &rb)
     // CTA and split them over more warps (rows per warp >= 8, a multiple of 4)
     nr = st.NR;
     rb = st.RB;
-    while (G * rb * 2 <= kTMaxCWarps && nr >= 16 && nr % 8 == 0) {
+    while (G * rb * 2 <= st.W && nr >= 16 && nr % 8 == 0) {
         nr /= 2;
         rb *= 2;
     }
