@@ -30,8 +30,9 @@ int main()
         g.hzPos = hz.data();
         HostGeometry hg;
         if (build_geometry(g, hg) != CTLAB_OK) return 3;
+        for (int wcap : {15, 7})
         for (int gcap : {16, 1}) {
-            const ProjTStaging st = proj_t_staging(hg, gcap);
+            const ProjTStaging st = proj_t_staging(hg, gcap, 0, 0, wcap);
             std::vector<int> all(PN);
             for (int i = 0; i < PN; ++i) all[i] = i;
             const ProjGroups pg = proj_t_make_groups(hg, all, st);
@@ -46,9 +47,9 @@ int main()
             }
             for (int c : seen) bad += c != 1;
             std::printf("%d %d ok=%d G=%d NR=%d RB=%d ZS=%d CB=%d KB=%d KR=%d nstage=%d smem=%zu groupsG=%d ngroups=%d "
-                        "table=%zu lnr=%d lrb=%d DNV=%d PN=%d badpos=%d\n",
+                        "table=%zu lnr=%d lrb=%d DNV=%d PN=%d badpos=%d W=%d\n",
                         idx, gcap, (int)st.ok, st.G, st.NR, st.RB, st.ZS, st.CB, st.KB, st.KR, st.nstage, st.smem, pg.G,
-                        pg.ngroups, pg.table.size(), nr, rb, DNV, PN, bad);
+                        pg.ngroups, pg.table.size(), nr, rb, DNV, PN, bad, st.W);
         }
     }
 }
