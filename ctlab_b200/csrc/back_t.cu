@@ -511,22 +511,24 @@ int e_pitch(int DNV, int zs) { return (zs * vpt_of(DNV, zs)) | 1; }
 // the largest (E, dE) pitch over the two block shapes
 int e_pitch_max(int DNV) { return std::max(std::max(e_pitch(DNV, 8), e_pitch(DNV, 16)), e_pitch(DNV, 4)); }
 
-// z segments per column: 4 (256 threads, two CTAs per SM), unless
-// CTLAB_BACKT_ZS=8 or 16 selects the 512- or 1024-thread shape.  All give
-// the same results.  On the B200 at 512x512x256 / 984 views: 52.1 ms (4),
-// 57.7 ms (8), 63.0 ms (16).  A warp's per-view bookkeeping (loop, waits,
-// slot addresses, phase-A set-up loads) is spread over the voxels of its
-// threads' segments, 64 / 32 / 16 of them; the 256-thread shape still runs
-// 16 warps per SM, as two independent CTAs whose barriers do not align.
+// z segments per column forced by CTLAB_BACKT_ZS (4, 8, 16), or 0: chosen
+// per launch (launch_shape).  All shapes give the same results.  On the
+// B200 at 512x512x256 / 984 views: 52.1 ms (4), 57.7 ms (8), 63.0 ms (16).
+// A warp's per-view bookkeeping (loop, waits, slot addresses, phase-A
+// set-up loads) is spread over the voxels of its threads' segments, 64 / 32
+// / 16 of them; the 256-thread shape still runs 16 warps per SM, as two
+// independent CTAs whose barriers do not align.
 int back_t_zs()
 {
     static const int zs = [] {
         const char *e = std::getenv("CTLAB_BACKT_ZS");
-        const int v = e ? std::atoi(e) : 4;
-        return (v == 8 || v == 16) ? v : 4;
+        const int v = e ? std::atoi(e) : 0;
+        return (v == 4 || v == 8 || v == 16) ? v : 0;
     }();
     return zs;
 }
+// views in a launch from which the 256-thread shape is used
+constexpr int kZs4Views = 192;
 
 size_t dyn_smem(int rmax, int vp, int es2, int ebuf = 2)
 {
@@ -589,8 +591,14 @@ __global__ void __launch_bounds__(256) zrange_kernel(BackArgs a, int zblk, int2 
     }
 }
 
+// With q set, a launch is not made: q receives the CTAs one launch of this
+// kernel keeps resident on the device and the CTAs of one brick row.
+struct BackLaunchQuery {
+    int resident = 0, ctas_per_row = 0;
+};
+
 template <int ZS, int KSEG, int VPT, bool ZSKIP>
-cudaError_t launch_k(const BackArgs &a, cudaStream_t s)
+cudaError_t launch_k(const BackArgs &a, cudaStream_t s, BackLaunchQuery *q)
 {
     const int es2 = e_pitch(a.DNV, ZS); // (E, dE) pairs per column, odd pitch
     const size_t sm = dyn_smem(a.rmax, a.vp, es2, ZS == 4 ? 1 : 2);
@@ -601,6 +609,15 @@ cudaError_t launch_k(const BackArgs &a, cudaStream_t s)
     if (a.by_off < 0 || a.by_count < 0 || (a.by_count == 0 && a.by_off != 0) || a.by_off + a.by_count > bys)
         return cudaErrorInvalidValue;
     dim3 grid((a.XN + kB - 1) / kB, a.by_count > 0 ? a.by_count : bys, (a.ZN + ZS * KSEG - 1) / (ZS * KSEG));
+    if (q) {
+        int dev = 0, sms = 0, per_sm = 0;
+        e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kCols * ZS, sm);
+        q->resident = sms * per_sm;
+        q->ctas_per_row = (int)(grid.x * grid.z);
+        return e;
+    }
     if (ZSKIP && a.zrange) {
         zrange_kernel<<<grid.z, 256, 0, s>>>(a, ZS * KSEG, a.zrange);
         e = cudaGetLastError();
@@ -615,28 +632,41 @@ cudaError_t launch_k(const BackArgs &a, cudaStream_t s)
 // skip the views whose cone misses it.  256 threads: segments up to 64
 // voxels; 512 threads: up to 32; 1024 threads: up to 16.
 template <int ZS, int VPT>
-cudaError_t launch_z(const BackArgs &a, cudaStream_t s)
+cudaError_t launch_z(const BackArgs &a, cudaStream_t s, BackLaunchQuery *q)
 {
     constexpr int KMAX = 256 / ZS;
-    if (a.ZN <= ZS * 4) return launch_k<ZS, 4, VPT, false>(a, s);
-    if (a.ZN <= ZS * 8) return launch_k<ZS, 8, VPT, false>(a, s);
-    if (ZS * 16 < 256 && a.ZN <= ZS * 16) return launch_k<ZS, 16, VPT, false>(a, s);
-    if (ZS * 32 < 256 && a.ZN <= ZS * 32) return launch_k<ZS, 32, VPT, false>(a, s);
-    if (a.zskip || a.ZN > 256) return launch_k<ZS, KMAX, VPT, true>(a, s);
-    return launch_k<ZS, KMAX, VPT, false>(a, s);
+    if (a.ZN <= ZS * 4) return launch_k<ZS, 4, VPT, false>(a, s, q);
+    if (a.ZN <= ZS * 8) return launch_k<ZS, 8, VPT, false>(a, s, q);
+    if (ZS * 16 < 256 && a.ZN <= ZS * 16) return launch_k<ZS, 16, VPT, false>(a, s, q);
+    if (ZS * 32 < 256 && a.ZN <= ZS * 32) return launch_k<ZS, 32, VPT, false>(a, s, q);
+    if (a.zskip || a.ZN > 256) return launch_k<ZS, KMAX, VPT, true>(a, s, q);
+    return launch_k<ZS, KMAX, VPT, false>(a, s, q);
 }
 
 template <int ZS>
-cudaError_t launch_vpt(const BackArgs &a, cudaStream_t s)
+cudaError_t launch_vpt(const BackArgs &a, cudaStream_t s, BackLaunchQuery *q)
 {
     switch (vpt_of(a.DNV, ZS)) {
-    case 2: return launch_z<ZS, 2>(a, s);
-    case 5: return launch_z<ZS, 5>(a, s);
-    case 9: return launch_z<ZS, 9>(a, s);
-    case 17: return launch_z<ZS, 17>(a, s);
-    case 33: return launch_z<ZS, 33>(a, s);
+    case 2: return launch_z<ZS, 2>(a, s, q);
+    case 5: return launch_z<ZS, 5>(a, s, q);
+    case 9: return launch_z<ZS, 9>(a, s, q);
+    case 17: return launch_z<ZS, 17>(a, s, q);
+    case 33: return launch_z<ZS, 33>(a, s, q);
     default: return cudaErrorInvalidValue;
     }
+}
+
+// The launch's block shape: CTLAB_BACKT_ZS=4, 8 or 16 forces it; otherwise
+// 256 threads (two CTAs per SM) for launches of many views and 512 threads
+// for short view lists (ordered subsets), where the 512-thread shape's
+// shorter per-CTA pipeline fill wins.
+cudaError_t launch_shape(const BackArgs &a, cudaStream_t s, BackLaunchQuery *q)
+{
+    int zs = back_t_zs();
+    if (zs == 0) zs = a.n >= kZs4Views ? 4 : 8;
+    if (zs == 4 && vpt_of(a.DNV, 4) == 0) zs = 8;
+    if (zs == 4) return launch_vpt<4>(a, s, q);
+    return zs == 16 ? launch_vpt<16>(a, s, q) : launch_vpt<8>(a, s, q);
 }
 
 } // namespace
@@ -709,13 +739,20 @@ cudaError_t launch_pv(const ProjSatArgs &a, float *out, int vp, cudaStream_t s)
     return cudaGetLastError();
 }
 
+cudaError_t back_t_query(const BackArgs &a, int *resident, int *ctas_per_row)
+{
+    BackLaunchQuery q;
+    cudaError_t e = a.n > 0 ? launch_shape(a, nullptr, &q) : cudaErrorInvalidValue;
+    *resident = q.resident;
+    *ctas_per_row = q.ctas_per_row;
+    return e;
+}
+
 cudaError_t launch_back_t(const BackArgs &a, cudaStream_t s, int *launches)
 {
     if (launches) ++*launches;
     if (a.n <= 0) return cudaSuccess;
-    const int zs = back_t_zs();
-    if (zs == 4 && vpt_of(a.DNV, 4) != 0) return launch_vpt<4>(a, s);
-    return zs == 16 ? launch_vpt<16>(a, s) : launch_vpt<8>(a, s);
+    return launch_shape(a, s, nullptr);
 }
 
 } // namespace ctlab

@@ -302,6 +302,9 @@ struct BackArgs {
 cudaError_t launch_back(const BackArgs &a, cudaStream_t s, int *launches);
 // Backprojector on projection v-prefixes (sat mode ZPREFIX).
 cudaError_t launch_back_t(const BackArgs &a, cudaStream_t s, int *launches);
+// Without launching: the CTAs the backprojector launch for `a` keeps resident
+// on the device (one wave) and its CTAs per brick row.
+cudaError_t back_t_query(const BackArgs &a, int *resident, int *ctas_per_row);
 bool back_t_supported(int DNV);
 int back_t_pitch(int DNV);
 int back_t_staging_rows(const HostGeometry &g);

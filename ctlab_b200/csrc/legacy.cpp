@@ -333,9 +333,18 @@ int legacy_back(LegacyCtx &c, const float *hprj, float *hvol, const unsigned cha
             if (rc == CTLAB_OK) CTLAB_CUDA_TRY(cudaStreamWaitEvent(s, c.ev[k], 0));
             if (rc == CTLAB_OK) rc = plan_proj_sat_range(p, p->d_all_views, v0, v1 - v0, c.d_prj, s);
         }
-        // the volume in y slabs of brick rows, each downloaded when done
+        // the volume in y slabs of brick rows, each downloaded when done; the
+        // slabs end on whole waves of the backprojector's CTAs, so a slab
+        // costs no more than the same rows inside one launch
         const int bys = (g.YN + 7) / 8;
-        const std::vector<int> bc = y_cuts(bys, 1);
+        int wave = 0;
+        if (rc == CTLAB_OK) rc = plan_back_wave_rows(p, g.PN, &wave);
+        std::vector<int> bc = {0};
+        for (int k = 1; k < kChunks && wave > 0; ++k) {
+            const int r = (int)std::lround((double)k * bys / kChunks / wave) * wave;
+            if (r > bc.back() && r < bys) bc.push_back(r);
+        }
+        bc.push_back(bys);
         for (size_t k = 0; k + 1 < bc.size() && rc == CTLAB_OK; ++k) {
             rc = plan_back_rows(p, p->d_all_views, g.PN, dm, c.d_vol, s, BACK_PLAIN, nullptr, 1.f, 0, 0.f, 0.f,
                                 bc[k], bc[k + 1] - bc[k]);

@@ -266,12 +266,10 @@ int plan_back_list(ctlab_plan *p, const int *d_list, int n, const unsigned char 
     return plan_back_rows(p, d_list, n, d_mask, d_vol, s, epilogue, col_sum, lambda, clamp, min_v, max_v, 0, 0);
 }
 
-int plan_back_rows(ctlab_plan *p, const int *d_list, int n, const unsigned char *d_mask, float *d_vol,
-                   cudaStream_t s, int epilogue, const float *col_sum, float lambda, int clamp, float min_v,
-                   float max_v, int by_off, int by_count)
+static BackArgs back_args(ctlab_plan *p, const int *d_list, int n, const unsigned char *d_mask, float *d_vol,
+                          int epilogue, const float *col_sum, float lambda, int clamp, float min_v, float max_v,
+                          int by_off, int by_count)
 {
-    if ((by_off != 0 || by_count != 0) && (p->sat_mode != CTLAB_SAT_ZPREFIX || n == 0))
-        return set_status(CTLAB_ERR_INTERNAL, "brick-row ranges need z-prefix mode and views");
     const HostGeometry &g = p->g;
     BackArgs a;
     std::memset(&a, 0, sizeof a);
@@ -305,6 +303,38 @@ int plan_back_rows(ctlab_plan *p, const int *d_list, int n, const unsigned char 
     a.by_count = by_count;
     for (const DevView &V : g.views)
         if (V.zP != g.views[0].zP) a.zskip = 1; // a helical scan
+    return a;
+}
+
+int plan_back_wave_rows(ctlab_plan *p, int n, int *rows)
+{
+    *rows = 0;
+    if (p->sat_mode != CTLAB_SAT_ZPREFIX || n <= 0) return CTLAB_OK;
+    const BackArgs a = back_args(p, p->d_all_views, n, nullptr, nullptr, BACK_PLAIN, nullptr, 1.f, 0, 0.f, 0.f, 0, 0);
+    int resident = 0, per_row = 0;
+    cudaError_t e = back_t_query(a, &resident, &per_row);
+    if (e != cudaSuccess) return cuda_status(e, "backprojector occupancy");
+    if (resident <= 0 || per_row <= 0) return CTLAB_OK;
+    // the fewest brick rows whose CTAs fill whole waves: lcm(per_row, resident) / per_row
+    long long a0 = per_row, b0 = resident;
+    while (b0) {
+        const long long t = a0 % b0;
+        a0 = b0;
+        b0 = t;
+    }
+    *rows = (int)(resident / a0);
+    return CTLAB_OK;
+}
+
+int plan_back_rows(ctlab_plan *p, const int *d_list, int n, const unsigned char *d_mask, float *d_vol,
+                   cudaStream_t s, int epilogue, const float *col_sum, float lambda, int clamp, float min_v,
+                   float max_v, int by_off, int by_count)
+{
+    if ((by_off != 0 || by_count != 0) && (p->sat_mode != CTLAB_SAT_ZPREFIX || n == 0))
+        return set_status(CTLAB_ERR_INTERNAL, "brick-row ranges need z-prefix mode and views");
+    const HostGeometry &g = p->g;
+    const BackArgs a = back_args(p, d_list, n, d_mask, d_vol, epilogue, col_sum, lambda, clamp, min_v, max_v, by_off,
+                                 by_count);
     if (n == 0 && epilogue == BACK_PLAIN) {
         CTLAB_CUDA_TRY(cudaMemsetAsync(d_vol, 0, sizeof(float) * (size_t)g.XN * g.YN * g.ZN, s));
         return CTLAB_OK;

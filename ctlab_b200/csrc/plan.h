@@ -80,6 +80,9 @@ int plan_upload_list(ctlab_plan *p, const int *h_views, int n, cudaStream_t s);
 int plan_volume_sat_rows(ctlab_plan *p, const float *d_vol, const unsigned char *d_mask, int y0, int y1,
                          cudaStream_t s);
 int plan_proj_sat_range(ctlab_plan *p, const int *d_list, int first, int n, const float *d_prj, cudaStream_t s);
+// The fewest brick rows whose backprojector CTAs (a launch of n views) fill
+// whole waves of the device, or 0 when unknown (not a z-prefix plan).
+int plan_back_wave_rows(ctlab_plan *p, int n, int *rows);
 int plan_back_rows(ctlab_plan *p, const int *d_list, int n, const unsigned char *d_mask, float *d_vol,
                    cudaStream_t s, int epilogue, const float *col_sum, float lambda, int clamp, float min_v,
                    float max_v, int by_off, int by_count);
