@@ -410,3 +410,49 @@ def test_legacy_overlapped_copies_equal_plan_path(torch_cuda, sat_mode, pinned, 
         torch.cuda.synchronize()
         np.testing.assert_array_equal(out.cpu().numpy(), hp)
         np.testing.assert_array_equal(vb.cpu().numpy(), hb)
+
+
+_SHAPE_SCRIPT = r"""
+import sys, json
+import numpy as np, torch
+sys.path.insert(0, sys.argv[1])
+import ctlab_b200 as cb, oracle
+from ctlab_b200 import geometry as G
+out = {}
+cases = {"small": dict(), "odd_offsets": dict(XN=23, YN=19, ZN=13, DNU=37, DNV=11, col_offset=0.37,
+         row_offset=-0.21, center=(1.3, -0.7, 0.4), start=0.05),
+         "helical_long": dict(PN=40, ZN=600, dz=0.05, zpos=np.linspace(-14.0, 14.0, 40)),
+         "many_views": dict(PN=240, ZN=40, DNV=20)}
+for name, kw in cases.items():
+    g = G.small(**kw)
+    rng = np.random.default_rng(3)
+    prj = rng.random(g.prj_shape).astype(np.float32)
+    ref = oracle.dd3_back(g, prj)
+    with cb.Plan(g) as plan:
+        v = torch.zeros(g.vol_shape, dtype=torch.float32, device="cuda")
+        plan.back(torch.from_numpy(prj).cuda(), v)
+        torch.cuda.synchronize()
+        got = v.cpu().numpy()
+    out[name] = float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
+print(json.dumps(out))
+"""
+
+
+@pytest.mark.parametrize("zs", ["4", "8", "16"])
+def test_backprojector_block_shapes_match_oracle(torch_cuda, zs):
+    """Every block shape of the z-prefix backprojector (CTLAB_BACKT_ZS forces one for the
+    whole process: 256, 512 or 1024 threads) on short and long view lists, odd sizes and a
+    long helical volume (z blocks skipped per view)."""
+    import json
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, CTLAB_BACKT_ZS=zs)
+    r = subprocess.run([sys.executable, "-c", _SHAPE_SCRIPT, root], env=env, capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    errs = json.loads(r.stdout.strip().splitlines()[-1])
+    for name, e in errs.items():
+        record_error(f"back/{name}/shape{zs}", e)
+        assert e <= REL_L2, (name, zs, e)
