@@ -286,6 +286,9 @@ def roofline_entry(dom, t_dom, alg, achieved, peak, peak_kind, clocks, args):
         r["issue_frac"] = c["warp_inst_per_launch"] / t / issue_peak
         r["counters_source"] = (f"profiles/kernel_counters.json ({c['profile']}, captured {c['captured']}; "
                                 f"kernel source {'unchanged' if c['source_matches'] else 'CHANGED'} since)")
+        # what actually limits the kernel: HBM when it moves a good part of the
+        # peak, otherwise instruction issue (and the latency issue-bound code waits on)
+        r["limiter"] = "hbm" if r["dram_frac"] >= 0.5 else "instruction issue"
     return r
 
 
