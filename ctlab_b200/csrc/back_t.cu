@@ -453,19 +453,41 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
     const long long colidx = (long long)y * a.XN + x;
     const float m = a.mask ? (a.mask[colidx] ? 1.f : 0.f) : 1.f;
     float *o = a.out + colidx * ZN;
+    if (a.epilogue == BACK_SART_UPDATE) {
+        // x = (x + lambda * acc / colSum) * mask, eight voxels at a time: their
+        // loads are issued together (the image and the column sums are read
+        // through different pointers, so the compiler would otherwise keep each
+        // load behind the previous voxel's store)
+        const float *cs_col = a.col_sum + colidx * ZN;
 #pragma unroll
-    for (int r = 0; r < KSEG; ++r) {
-        const int k = k0 + r;
-        if (k < ZN) {
-            if (a.epilogue == BACK_SART_UPDATE) {
-                const float cs = a.col_sum[colidx * ZN + k];
-                const float upd = (cs > 1.0e-7f) ? acc[r] / cs : 0.f;
-                float v = (o[k] + a.lambda * upd) * m;
-                if (a.clamp) v = fminf(fmaxf(v, a.min_v), a.max_v);
-                o[k] = v;
-            } else {
-                o[k] = acc[r] * m;
+        for (int r0 = 0; r0 < KSEG; r0 += 8) {
+            float cs[8], xv[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int k = k0 + r0 + q;
+                cs[q] = 0.f;
+                xv[q] = 0.f;
+                if (r0 + q < KSEG && k < ZN) {
+                    cs[q] = __ldg(cs_col + k);
+                    xv[q] = o[k];
+                }
             }
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int k = k0 + r0 + q;
+                if (r0 + q < KSEG && k < ZN) {
+                    const float upd = (cs[q] > 1.0e-7f) ? acc[r0 + q] / cs[q] : 0.f;
+                    float v = (xv[q] + a.lambda * upd) * m;
+                    if (a.clamp) v = fminf(fmaxf(v, a.min_v), a.max_v);
+                    o[k] = v;
+                }
+            }
+        }
+    } else {
+#pragma unroll
+        for (int r = 0; r < KSEG; ++r) {
+            const int k = k0 + r;
+            if (k < ZN) o[k] = acc[r] * m;
         }
     }
 }
