@@ -576,8 +576,9 @@ def run_recon(args):
     iterations) at 256x256x128 / 720 views / 384x128 detector from the projection of a
     seeded random-ellipsoid phantom with Poisson noise at I0 = 1e5 photons per ray:
     b = -ln(max(Poisson(I0 exp(-Ax)), 1) / I0).  Device times with CUDA events (the
-    solves without per-iteration residuals), then the residual ||Ax - b||/||b|| and the
-    RMSE against the phantom after every iteration from a second, untimed pass."""
+    solves without per-iteration residuals, after one warm-up call that builds each
+    solver's workspace and weights), then the residual ||Ax - b||/||b|| and the RMSE
+    against the phantom after every iteration from a second, untimed pass."""
     import torch
 
     import ctlab_b200 as cb
@@ -622,6 +623,10 @@ def run_recon(args):
         return res, rmse
 
     n_os, n_fi = (args.recon_iters, args.recon_iters) if args.recon_iters else (30, 50)
+    # one warm-up call of each solver builds its workspace and SART weights
+    # on the plan (once per plan and mask); the timed calls reuse them
+    plan.os_sart(torch.zeros_like(truth), meas, os_num=24, iter_num=1)
+    plan.fista_tv(torch.zeros_like(truth), meas, iter_num=1, tv_lambda=1e-4)
     with ClockSampler(local) as clk:
         os_ms, _ = timed(lambda x, n: plan.os_sart(x, meas, os_num=24, iter_num=n_os))
         fi_ms, _ = timed(lambda x, n: plan.fista_tv(x, meas, iter_num=n_fi, tv_lambda=1e-4))

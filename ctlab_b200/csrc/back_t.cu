@@ -18,16 +18,20 @@
 //   phase A    per column and detector row boundary v', the strip integral
 //              between the column's two u boundaries,
 //                 E_c(v') = sg * [ sum of P over whole cells + f_b P_b - f_a P_a ],
-//              sg orienting it like the voxel's z axis (FP32), stored with its
-//              forward difference as (E, dE) pairs; ZS threads per column
-//              each run a contiguous stretch of rows with a warp-uniform trip
-//              count, from a strip set-up computed two views ahead;
+//              sg orienting it like the voxel's z axis (FP32), stored per row
+//              i as the affine form of its linear piece in vn = v / DNV,
+//                 (E_c(i) - i dE_i, DNV dE_i),  dE_i = E_c(i+1) - E_c(i),
+//              so that E_c(v) = first + vn * second on [i, i+1]; ZS
+//              threads per column each run a contiguous stretch of rows with
+//              a warp-uniform trip count, from a strip set-up computed two
+//              views ahead;
 //   phase B    each voxel boundary k samples E_c linearly at
 //              v = DNV * sat(V0 + V1 k) with one 64-bit shared load and the
 //              voxel accumulates E_c(v_{k+1}) - E_c(v_k): one saturating FMA
 //              clamps, the round-toward-zero FMA with 2^23 gives floor(v)
 //              biased for the shared-memory address -- no float/int
-//              conversions.
+//              conversions -- and one FMA evaluates the piece (7
+//              instructions per boundary).
 // In the 512- and 1024-thread shapes E is double buffered, so one barrier per
 // view separates A(l) from B(l) and the issue of view l+2's copy; the
 // 256-thread shape keeps one E table and a second barrier after B(l), the
@@ -93,12 +97,21 @@ __device__ __forceinline__ void unroll_for(F &&f)
     }
 }
 
+// The table entry of row i from E(i) and E(i+1): the piece E(i) + (v - i) dE
+// as an affine function of vn = v / DNV.
+__device__ __forceinline__ float2 affine_piece(float e, float en, float fi, float dnv)
+{
+    const float d = en - e;
+    return make_float2(fmaf(-fi, d, e), dnv * d);
+}
+
 // Phase A run of one thread: E at rows i0 .. i0+VPT of one column from the
 // staged P rows pa, pb (and NX whole cells pm[] between them), stored as VPT
-// (E, dE) pairs at eout.  Every address carries i0; offsets are immediates.
+// affine pieces at eout (nfi0 = -i0).  Every address carries i0; offsets are
+// immediates.
 template <int VPT, int NX>
 __device__ __forceinline__ void phase_a_run(uint32_t pa, uint32_t pb, const uint32_t (&pm)[3], const float (&wmv)[3],
-                                            float wa, float wb, uint32_t eout)
+                                            float wa, float wb, float nfi0, float dnv, uint32_t eout)
 {
     float e_prev = 0.f;
     unroll_for<0, VPT + 1>([&](auto jt) {
@@ -108,7 +121,13 @@ __device__ __forceinline__ void phase_a_run(uint32_t pa, uint32_t pb, const uint
             constexpr int m = decltype(mt)::value;
             e = fmaf(wmv[m], lds_f32_at<4 * j>(pm[m]), e);
         });
-        if constexpr (j > 0) sts_f32x2_at<8 * (j - 1)>(eout, e_prev, e - e_prev);
+        if constexpr (j > 0) {
+            // first = E(i) - i d with i = i0 + j - 1
+            const float d = e - e_prev;
+            float first = fmaf(nfi0, d, e_prev);
+            if constexpr (j > 1) first = fmaf(-(float)(j - 1), d, first);
+            sts_f32x2_at<8 * (j - 1)>(eout, first, dnv * d);
+        }
         e_prev = e;
     });
 }
@@ -319,6 +338,7 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
     const int ac = tid / kAPh, aph = tid % kAPh;
     const int acx = ac & (kB - 1), acy = ac / kB;
     const int i0 = aph * VPT; // this thread's entries i0 .. i0+VPT-1 (kAPh*VPT > DNV)
+    const float nfi0 = -(float)i0;
 
     for (int li = 0; li < n; ++li) {
         const int b = li & 1, ls = li % kGeo;
@@ -344,7 +364,7 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
             st.ia = min((int)uca, DNU - 1);
             st.ib = min((int)ucb, DNU - 1);
             const float fa = (float)(uca - st.ia), fb = (float)(ucb - st.ib);
-            const float sg = ((ub - ua > 0) ? 1.f : -1.f) * ((s_V1[ls][ac] > 0.f) ? 1.f : -1.f);
+            const float sgn = ((ub - ua > 0) ? 1.f : -1.f) * ((s_V1[ls][ac] > 0.f) ? 1.f : -1.f);
             const int dc = st.ib - st.ia;
             float wa, wb;
             if (dc == 0) {
@@ -357,12 +377,12 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
                 wa = -fa;
                 wb = fb - 1.f;
             }
-            st.wa = wa * sg;
-            st.wb = wb * sg;
+            st.wa = wa * sgn;
+            st.wb = wb * sgn;
             // whole cells strictly between a and b
             st.nm = max(abs(dc) - 1, 0);
             st.first = min(st.ia, st.ib) + 1;
-            st.wm = dc > 0 ? sg : -sg;
+            st.wm = dc > 0 ? sgn : -sgn;
             return st;
         };
 
@@ -382,10 +402,10 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
             const int nmax = (int)__reduce_max_sync(0xffffffffu, q2.z);
             const uint32_t eout = E2_addr + 8u * (uint32_t)((eb * kCols + ac) * es2 + i0);
             switch (nmax) {
-            case 0: phase_a_run<VPT, 0>(pa, pb, pm, wmv, wa, wb, eout); break;
-            case 1: phase_a_run<VPT, 1>(pa, pb, pm, wmv, wa, wb, eout); break;
-            case 2: phase_a_run<VPT, 2>(pa, pb, pm, wmv, wa, wb, eout); break;
-            case 3: phase_a_run<VPT, 3>(pa, pb, pm, wmv, wa, wb, eout); break;
+            case 0: phase_a_run<VPT, 0>(pa, pb, pm, wmv, wa, wb, nfi0, DNVf, eout); break;
+            case 1: phase_a_run<VPT, 1>(pa, pb, pm, wmv, wa, wb, nfi0, DNVf, eout); break;
+            case 2: phase_a_run<VPT, 2>(pa, pb, pm, wmv, wa, wb, nfi0, DNVf, eout); break;
+            case 3: phase_a_run<VPT, 3>(pa, pb, pm, wmv, wa, wb, nfi0, DNVf, eout); break;
             default: {
                 // cells much wider than voxels: the whole cells by a loop
                 const Strip st = strip();
@@ -398,7 +418,7 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
                     const uint32_t o = 4u * (uint32_t)j;
                     float en = fmaf(st.wb, lds_f32(row(st.ib) + o), st.wa * lds_f32(row(st.ia) + o));
                     for (int m = 0; m < st.nm; ++m) en = fmaf(st.wm, lds_f32(row(st.first + m) + o), en);
-                    if (j > 0) Ec[i0 + j - 1] = make_float2(e, en - e);
+                    if (j > 0) Ec[i0 + j - 1] = affine_piece(e, en, (float)(i0 + j - 1), DNVf);
                     e = en;
                 }
             }
@@ -416,7 +436,7 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
             float e = eval(i0);
             for (int j = 0; j < VPT; ++j) {
                 const float en = eval(i0 + j + 1);
-                Ec[i0 + j] = make_float2(e, en - e);
+                Ec[i0 + j] = affine_piece(e, en, (float)(i0 + j), DNVf);
                 e = en;
             }
         }
@@ -438,9 +458,8 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
             for (int r = 0; r <= KSEG; ++r) {
                 const float vn = __saturatef(fmaf(V1, (float)r, vb0));
                 const float rr = __fmaf_rz(vn, DNVf, 8388608.f); // 2^23 + floor(DNV vn)
-                const float fz = fmaf(vn, DNVf, 8388608.f - rr);
-                const float2 ed = lds_f32x2(__float_as_uint(rr) * 8u + base);
-                const float ev = fmaf(fz, ed.y, ed.x);
+                const float2 pc = lds_f32x2(__float_as_uint(rr) * 8u + base);
+                const float ev = fmaf(vn, pc.y, pc.x); // E_c(DNV vn)
                 if (r > 0) acc[r - 1] += ev - prev;
                 prev = ev;
             }

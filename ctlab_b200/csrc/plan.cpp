@@ -77,7 +77,9 @@ void plan_free(ctlab_plan *p)
         if (b) cudaFree(b);
     for (auto &e : p->ev)
         if (e) cudaEventDestroy(e);
-    sart_work_free(p->sart);
+    solver_work_free(p->sart);
+    solver_work_free(p->fista);
+    solver_work_free(p->cg);
     delete p;
 }
 

@@ -7,7 +7,7 @@
 #include "internal.h"
 
 namespace ctlab {
-struct SartWork; // OS-SART workspace and weights kept between calls (recon.cpp)
+struct SolverWork; // solver workspace and weights kept between calls (recon.cpp)
 }
 
 struct ctlab_plan {
@@ -46,7 +46,7 @@ struct ctlab_plan {
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
     int last_launches = 0;
     long long bytes = 0;
-    ctlab::SartWork *sart = nullptr;
+    ctlab::SolverWork *sart = nullptr, *fista = nullptr, *cg = nullptr; // per solver
     std::mutex mu;
 };
 
@@ -59,7 +59,7 @@ struct GroupTab {
 };
 
 void plan_free(ctlab_plan *p);
-void sart_work_free(SartWork *w);
+void solver_work_free(SolverWork *w);
 // Groups the host list (positions into a device view list) and uploads the
 // table to d_dst (capacity cap ints); synchronous.
 int plan_groups(ctlab_plan *p, const std::vector<int> &host_list, int *d_dst, int cap, GroupTab &out,

@@ -18,26 +18,6 @@ using namespace ctlab;
 
 namespace {
 
-struct DevBuf {
-    void *p = nullptr;
-    ~DevBuf()
-    {
-        if (p) cudaFree(p);
-    }
-    template <class T>
-    T *as()
-    {
-        return (T *)p;
-    }
-};
-
-int alloc(DevBuf &b, size_t bytes)
-{
-    cudaError_t e = cudaMalloc(&b.p, bytes ? bytes : 1);
-    if (e != cudaSuccess) return cuda_status(e, "reconstruction workspace");
-    return CTLAB_OK;
-}
-
 // ||b - A x|| / ||b|| for the current x over the views of d_order (all PN).
 int exact_residual(ctlab_plan *p, const float *d_x, const unsigned char *d_mask, const int *d_order,
                    const GroupTab &gt, const float *d_bsub, float *d_est, double *d_acc, cudaStream_t s, float *out)
@@ -61,33 +41,36 @@ int exact_residual(ctlab_plan *p, const float *d_x, const unsigned char *d_mask,
 
 namespace ctlab {
 
-// OS-SART state kept on a plan between ctlab_os_sart calls: the buffers (so
-// repeated solves allocate nothing) and the view order, group tables and
-// SART weights (rowSum = A 1, colSum_s = B_s 1) of the last subsets and mask
-// used, identified by a hash of os_num, the order and the mask bytes.
-struct SartWork {
+// Solver state kept on a plan between calls of one solver (OS-SART,
+// FISTA-TV or CG): the buffers, so that repeated solves allocate nothing, and
+// for the SART-weighted solvers the view order, group tables and SART
+// weights (rowSum = A 1, colSum_s = B_s 1) of the last subsets and mask used,
+// identified by a hash of the subset count, the order and the mask bytes.
+struct SolverWork {
     unsigned long long key = 0;
     bool weights = false; // rows / cols hold the weights of `key`
     std::vector<GroupTab> gtab;
     struct Buf {
         void *p = nullptr;
         size_t cap = 0;
-    } order, groups, bsub, rows, cols, r, ones, acc, est;
-    ~SartWork()
+    } order, groups, bsub, rows, cols, r, ones, acc, est, vol[5];
+    ~SolverWork()
     {
         for (Buf *b : {&order, &groups, &bsub, &rows, &cols, &r, &ones, &acc, &est})
             if (b->p) cudaFree(b->p);
+        for (Buf &b : vol)
+            if (b.p) cudaFree(b.p);
     }
 };
 
-void sart_work_free(SartWork *w) { delete w; }
+void solver_work_free(SolverWork *w) { delete w; }
 
 } // namespace ctlab
 
 namespace {
 
 // Grows b to at least `bytes`; reports whether it was reallocated.
-int reserve(SartWork::Buf &b, size_t bytes, bool *moved)
+int reserve(SolverWork::Buf &b, size_t bytes, bool *moved)
 {
     if (bytes <= b.cap && b.p) return CTLAB_OK;
     if (b.p) cudaFree(b.p);
@@ -122,6 +105,28 @@ unsigned long long sart_key(const ctlab_plan *p, int os_num, const std::vector<i
     add(&m, 1);
     add(mask.data(), mask.size());
     return h;
+}
+
+// The plan's workspace slot *slot, created on first use.
+int solver_work(SolverWork **slot, SolverWork **out)
+{
+    if (!*slot) {
+        *slot = new (std::nothrow) SolverWork();
+        if (!*slot) return set_status(CTLAB_ERR_OOM, "host allocation failed");
+    }
+    *out = *slot;
+    return CTLAB_OK;
+}
+
+// The in-plane mask's bytes (empty without a mask); synchronous.
+int mask_bytes(const ctlab_plan *p, const unsigned char *d_mask, cudaStream_t s, std::vector<unsigned char> &out)
+{
+    out.clear();
+    if (!d_mask) return CTLAB_OK;
+    out.resize((size_t)p->g.XN * p->g.YN);
+    CTLAB_CUDA_TRY(cudaMemcpyAsync(out.data(), d_mask, out.size(), cudaMemcpyDeviceToHost, s));
+    CTLAB_CUDA_TRY(cudaStreamSynchronize(s));
+    return CTLAB_OK;
 }
 
 } // namespace
@@ -172,19 +177,14 @@ int ctlab_os_sart(ctlab_plan *plan, float *d_x, const float *d_meas, const unsig
     const int gcap = plan->groups_cap;
     // the mask's bytes identify the weights (a caller may rewrite a mask in place)
     std::vector<unsigned char> hmask;
-    if (d_mask) {
-        hmask.resize((size_t)g.XN * g.YN);
-        CTLAB_CUDA_TRY(cudaMemcpyAsync(hmask.data(), d_mask, hmask.size(), cudaMemcpyDeviceToHost, s));
-        CTLAB_CUDA_TRY(cudaStreamSynchronize(s));
-    }
+    SolverWork *wp = nullptr;
+    int rc = mask_bytes(plan, d_mask, s, hmask);
+    if (rc == CTLAB_OK) rc = solver_work(&plan->sart, &wp);
+    if (rc != CTLAB_OK) return rc;
     const unsigned long long key = sart_key(plan, os_num, order, hmask, d_mask != nullptr);
-    if (!plan->sart) {
-        plan->sart = new (std::nothrow) SartWork();
-        if (!plan->sart) return set_status(CTLAB_ERR_OOM, "host allocation failed");
-    }
-    SartWork &W = *plan->sart;
+    SolverWork &W = *wp;
     bool moved = false;
-    int rc = reserve(W.order, sizeof(int) * g.PN, &moved);
+    rc = reserve(W.order, sizeof(int) * g.PN, &moved);
     if (rc == CTLAB_OK) rc = reserve(W.groups, sizeof(int) * (size_t)gcap * (os_num + 1), &moved);
     if (rc == CTLAB_OK) rc = reserve(W.rows, sizeof(float) * nd * g.PN, &moved);
     if (rc == CTLAB_OK) rc = reserve(W.cols, sizeof(float) * nv * os_num, &moved);
@@ -275,46 +275,64 @@ int ctlab_fista_tv(ctlab_plan *plan, float *d_x, const float *d_meas, const unsi
     const long long nv = (long long)g.XN * g.YN * g.ZN;
     const int *all = plan->d_all_views;
 
-    DevBuf d_rows, d_cols, d_r, d_ones, d_y, d_xk, d_xp, d_g, d_acc, d_est;
-    int rc = alloc(d_rows, sizeof(float) * nd);
-    if (rc == CTLAB_OK) rc = alloc(d_cols, sizeof(float) * nv);
-    if (rc == CTLAB_OK) rc = alloc(d_r, sizeof(float) * nd);
-    if (rc == CTLAB_OK) rc = alloc(d_ones, sizeof(float) * std::max(nd, nv));
-    if (rc == CTLAB_OK) rc = alloc(d_y, sizeof(float) * nv);
-    if (rc == CTLAB_OK) rc = alloc(d_xk, sizeof(float) * nv);
-    if (rc == CTLAB_OK) rc = alloc(d_xp, sizeof(float) * nv);
-    if (rc == CTLAB_OK) rc = alloc(d_g, sizeof(float) * nv);
-    if (rc == CTLAB_OK) rc = alloc(d_acc, sizeof(double) * 2);
-    if (rc == CTLAB_OK && h_resid) rc = alloc(d_est, sizeof(float) * nd);
+    // workspace and SART weights (rowSum = A 1, colSum = B 1 over all views)
+    // kept on the plan, the weights identified by the mask's bytes
+    std::vector<unsigned char> hmask;
+    SolverWork *wp = nullptr;
+    int rc = mask_bytes(plan, d_mask, s, hmask);
+    if (rc == CTLAB_OK) rc = solver_work(&plan->fista, &wp);
     if (rc != CTLAB_OK) return rc;
+    SolverWork &W = *wp;
+    const unsigned long long key = sart_key(plan, 1, std::vector<int>(), hmask, d_mask != nullptr);
+    bool moved = false;
+    rc = reserve(W.rows, sizeof(float) * nd, &moved);
+    if (rc == CTLAB_OK) rc = reserve(W.cols, sizeof(float) * nv, &moved);
+    if (rc == CTLAB_OK) rc = reserve(W.r, sizeof(float) * nd, nullptr);
+    if (rc == CTLAB_OK) rc = reserve(W.ones, sizeof(float) * std::max(nd, nv), nullptr);
+    for (int k = 0; k < 4 && rc == CTLAB_OK; ++k) rc = reserve(W.vol[k], sizeof(float) * nv, nullptr);
+    if (rc == CTLAB_OK) rc = reserve(W.acc, sizeof(double) * 2, nullptr);
+    if (rc == CTLAB_OK && h_resid) rc = reserve(W.est, sizeof(float) * nd, nullptr);
+    if (rc != CTLAB_OK) {
+        W.weights = false;
+        return rc;
+    }
+    float *d_rows = (float *)W.rows.p, *d_cols = (float *)W.cols.p, *d_r = (float *)W.r.p;
+    float *d_ones = (float *)W.ones.p, *d_g = (float *)W.vol[3].p, *d_est = (float *)W.est.p;
+    double *d_acc = (double *)W.acc.p;
 
-    CTLAB_CUDA_TRY(launch_fill(d_ones.as<float>(), 1.f, std::max(nd, nv), s));
-    rc = plan_volume_sat(plan, d_ones.as<float>(), d_mask, s);
-    if (rc == CTLAB_OK)
-        rc = plan_proj_list(plan, all, g.PN, plan_all_groups(plan), d_rows.as<float>(), s, PROJ_PLAIN, nullptr, nullptr,
-                            nullptr);
-    if (rc == CTLAB_OK) rc = plan_proj_sat(plan, all, g.PN, d_ones.as<float>(), s);
-    if (rc == CTLAB_OK)
-        rc = plan_back_list(plan, all, g.PN, d_mask, d_cols.as<float>(), s, BACK_PLAIN, nullptr, 1.f, 0, 0.f, 0.f);
-    if (rc != CTLAB_OK) return rc;
-    CTLAB_CUDA_TRY(cudaMemcpyAsync(d_y.p, d_x, sizeof(float) * nv, cudaMemcpyDeviceToDevice, s));
-    CTLAB_CUDA_TRY(cudaMemcpyAsync(d_xp.p, d_x, sizeof(float) * nv, cudaMemcpyDeviceToDevice, s));
+    if (moved || !W.weights || W.key != key) {
+        W.weights = false;
+        CTLAB_CUDA_TRY(launch_fill(d_ones, 1.f, std::max(nd, nv), s));
+        rc = plan_volume_sat(plan, d_ones, d_mask, s);
+        if (rc == CTLAB_OK)
+            rc = plan_proj_list(plan, all, g.PN, plan_all_groups(plan), d_rows, s, PROJ_PLAIN, nullptr, nullptr,
+                                nullptr);
+        if (rc == CTLAB_OK) rc = plan_proj_sat(plan, all, g.PN, d_ones, s);
+        if (rc == CTLAB_OK)
+            rc = plan_back_list(plan, all, g.PN, d_mask, d_cols, s, BACK_PLAIN, nullptr, 1.f, 0, 0.f, 0.f);
+        // kept only once the device error word is clear
+        if (rc == CTLAB_OK) rc = plan_check_device_error(plan, s);
+        if (rc != CTLAB_OK) return rc;
+        W.key = key;
+        W.weights = true;
+    }
+    float *xk = (float *)W.vol[0].p, *xp = (float *)W.vol[1].p, *y = (float *)W.vol[2].p;
+    CTLAB_CUDA_TRY(cudaMemcpyAsync(y, d_x, sizeof(float) * nv, cudaMemcpyDeviceToDevice, s));
+    CTLAB_CUDA_TRY(cudaMemcpyAsync(xp, d_x, sizeof(float) * nv, cudaMemcpyDeviceToDevice, s));
 
     float t = 1.f;
-    float *xk = d_xk.as<float>(), *xp = d_xp.as<float>(), *y = d_y.as<float>();
     for (int it = 0; it < iter_num; ++it) {
         rc = plan_volume_sat(plan, y, d_mask, s);
         if (rc == CTLAB_OK)
-            rc = plan_proj_list(plan, all, g.PN, plan_all_groups(plan), d_r.as<float>(), s, PROJ_SART_RESIDUAL, d_meas,
-                                d_rows.as<float>(), nullptr);
-        if (rc == CTLAB_OK) rc = plan_proj_sat(plan, all, g.PN, d_r.as<float>(), s);
+            rc = plan_proj_list(plan, all, g.PN, plan_all_groups(plan), d_r, s, PROJ_SART_RESIDUAL, d_meas, d_rows,
+                                nullptr);
+        if (rc == CTLAB_OK) rc = plan_proj_sat(plan, all, g.PN, d_r, s);
         // z = (y + B r / colSum) * mask, in place in y
         if (rc == CTLAB_OK)
-            rc = plan_back_list(plan, all, g.PN, d_mask, y, s, BACK_SART_UPDATE, d_cols.as<float>(), 1.f, 0, 0.f,
-                                0.f);
+            rc = plan_back_list(plan, all, g.PN, d_mask, y, s, BACK_SART_UPDATE, d_cols, 1.f, 0, 0.f, 0.f);
         if (rc != CTLAB_OK) return rc;
-        CTLAB_CUDA_TRY(launch_tv_gradient(y, d_g.as<float>(), g.XN, g.YN, g.ZN, tv_eps, s));
-        CTLAB_CUDA_TRY(launch_tv_step(xk, y, d_g.as<float>(), d_mask, tv_lambda, nv, g.ZN, s));
+        CTLAB_CUDA_TRY(launch_tv_gradient(y, d_g, g.XN, g.YN, g.ZN, tv_eps, s));
+        CTLAB_CUDA_TRY(launch_tv_step(xk, y, d_g, d_mask, tv_lambda, nv, g.ZN, s));
         const float tn = 0.5f * (1.f + std::sqrt(1.f + 4.f * t * t));
         CTLAB_CUDA_TRY(cudaMemcpyAsync(y, xk, sizeof(float) * nv, cudaMemcpyDeviceToDevice, s));
         CTLAB_CUDA_TRY(launch_fista_step(xp, y, t, tn, nv, min_v, max_v, s));
@@ -322,8 +340,7 @@ int ctlab_fista_tv(ctlab_plan *plan, float *d_x, const float *d_meas, const unsi
         std::swap(xk, xp); // xp now holds x_k
         t = tn;
         if (h_resid) {
-            rc = exact_residual(plan, xp, d_mask, all, plan_all_groups(plan), d_meas, d_est.as<float>(),
-                                d_acc.as<double>(), s, h_resid + it);
+            rc = exact_residual(plan, xp, d_mask, all, plan_all_groups(plan), d_meas, d_est, d_acc, s, h_resid + it);
             if (rc != CTLAB_OK) return rc;
         }
     }
@@ -349,17 +366,19 @@ int ctlab_cg(ctlab_plan *plan, float *d_x, const float *d_meas, const unsigned c
     const long long nv = (long long)g.XN * g.YN * g.ZN;
     const int *all = plan->d_all_views;
 
-    DevBuf d_r, d_q, d_g, d_gn, d_d, d_acc;
-    int rc = alloc(d_r, sizeof(float) * nd);
-    if (rc == CTLAB_OK) rc = alloc(d_q, sizeof(float) * nd);
-    if (rc == CTLAB_OK) rc = alloc(d_g, sizeof(float) * nv);
-    if (rc == CTLAB_OK) rc = alloc(d_gn, sizeof(float) * nv);
-    if (rc == CTLAB_OK) rc = alloc(d_d, sizeof(float) * nv);
-    if (rc == CTLAB_OK) rc = alloc(d_acc, sizeof(double) * 4);
+    // workspace kept on the plan (repeated solves allocate nothing)
+    SolverWork *wp = nullptr;
+    int rc = solver_work(&plan->cg, &wp);
     if (rc != CTLAB_OK) return rc;
-    float *r = d_r.as<float>(), *q = d_q.as<float>(), *gk = d_g.as<float>(), *gn = d_gn.as<float>(),
-          *dk = d_d.as<float>();
-    double *acc = d_acc.as<double>();
+    SolverWork &W = *wp;
+    rc = reserve(W.r, sizeof(float) * nd, nullptr);
+    if (rc == CTLAB_OK) rc = reserve(W.est, sizeof(float) * nd, nullptr);
+    for (int k = 0; k < 3 && rc == CTLAB_OK; ++k) rc = reserve(W.vol[k], sizeof(float) * nv, nullptr);
+    if (rc == CTLAB_OK) rc = reserve(W.acc, sizeof(double) * 4, nullptr);
+    if (rc != CTLAB_OK) return rc;
+    float *r = (float *)W.r.p, *q = (float *)W.est.p, *gk = (float *)W.vol[0].p, *gn = (float *)W.vol[1].p,
+          *dk = (float *)W.vol[2].p;
+    double *acc = (double *)W.acc.p;
 
     // A v (masked volume) and A^T p (masked), over all views
     auto proj = [&](const float *vol, float *out) {

@@ -264,7 +264,9 @@ int ctlab_os_sart(ctlab_plan *plan, float *d_x, const float *d_meas, const unsig
  * one TV-gradient step of weight tv_lambda (smoothing tv_eps), FISTA
  * momentum clamped to [min_v, max_v] (FISTA_functor,
  * src/FastIterativeShrinkageAlgorithm.h:17-42).  h_resid as for
- * ctlab_os_sart. */
+ * ctlab_os_sart.  The plan keeps the call's workspace and SART weights
+ * (rowSum = A 1, colSum = B 1 over all views); a later call with the same
+ * mask bytes reuses them without allocating. */
 int ctlab_fista_tv(ctlab_plan *plan, float *d_x, const float *d_meas,
                    const unsigned char *d_mask, int iter_num, float tv_lambda, float tv_eps,
                    float min_v, float max_v, float *h_resid, void *stream);
@@ -275,7 +277,8 @@ int ctlab_fista_tv(ctlab_plan *plan, float *d_x, const float *d_meas,
  * (Crowder-Wolfe, the Hestenes-Stiefel form), _DI (Dixon) or _DY
  * (Dai-Yuan), the members of CGMethod, src/DD3_GPU_recon.h:14-19.  d_x holds
  * the initial image and receives the result; h_resid (may be NULL) receives
- * ||A x_k - b|| / ||b|| after each iteration.  Replaces the GPU body of CG,
+ * ||A x_k - b|| / ||b|| after each iteration.  The plan keeps the call's
+ * workspace for later calls.  Replaces the GPU body of CG,
  * src/DD3_GPU_recon.h:98-103. */
 #define CTLAB_CG_FR 0
 #define CTLAB_CG_PRP 1

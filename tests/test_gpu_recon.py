@@ -249,3 +249,37 @@ def test_os_sart_calls_reuse_weights_only_for_the_same_subsets_and_mask(torch_cu
         torch.cuda.synchronize()
     for got, want in zip((x_b, x_c, x_d), refs):
         assert torch.equal(got, want)
+
+
+def test_fista_tv_and_cg_calls_reuse_their_workspace(torch_cuda):
+    """FISTA-TV and CG keep their workspaces on the plan: a second call gives
+    the first call's result bit for bit, and a mask rewritten in place between
+    FISTA-TV calls gives what a fresh plan gives (its SART weights are rebuilt)."""
+    torch = torch_cuda
+    g, truth, prj = scan(4)
+    meas = dev(torch, prj)
+    mask_a = np.ones(g.XN * g.YN, np.uint8)
+    mask_b = (np.random.default_rng(5).random(g.XN * g.YN) > 0.3).astype(np.uint8)
+    with cb.Plan(g) as plan:
+        m = dev(torch, mask_a)
+        xs = []
+        for _ in range(2):
+            x = torch.zeros(g.vol_shape, dtype=torch.float32, device="cuda")
+            plan.fista_tv(x, meas, m, iter_num=3, tv_lambda=1e-3)
+            xs.append(x)
+        cgs = []
+        for _ in range(2):
+            x = torch.zeros(g.vol_shape, dtype=torch.float32, device="cuda")
+            plan.cg(x, meas, m, iter_num=3, method=1)
+            cgs.append(x)
+        m.copy_(dev(torch, mask_b))
+        x_b = torch.zeros(g.vol_shape, dtype=torch.float32, device="cuda")
+        plan.fista_tv(x_b, meas, m, iter_num=3, tv_lambda=1e-3)
+        torch.cuda.synchronize()
+    assert torch.equal(xs[0], xs[1]) and torch.equal(cgs[0], cgs[1])
+    assert float(xs[0].abs().max()) > 0
+    with cb.Plan(g) as fresh:
+        want = torch.zeros(g.vol_shape, dtype=torch.float32, device="cuda")
+        fresh.fista_tv(want, meas, dev(torch, mask_b), iter_num=3, tv_lambda=1e-3)
+        torch.cuda.synchronize()
+    assert torch.equal(x_b, want)
