@@ -125,16 +125,18 @@ cudaError_t launch_volume_sat(const float *vol, const unsigned char *mask, int X
                               int orientation, void *out, int zp, int f32pair, ScanState st,
                               int chunk, cudaStream_t s);
 
-// Slice-major column z-prefixes of the masked volume for one driving axis:
-// out[j][k][c] = sum_{z<k} f(column c of slice j, z), k in [0, ZN], FP64
-// sums rounded to FP32, row stride rs >= nb (pad columns zero).
+// Slice-major column z-prefixes of the masked volume for one driving axis,
+// as (prefix, slope) pairs: out[j][k][c] = (Z, f) with
+// Z = sum_{z<k} f(column c of slice j, z) (FP64 sums rounded to FP32) and
+// f = f(column c of slice j, k) (0 for k = ZN), k in [0, ZN]; row stride
+// rs >= nb pairs (pad columns zero).  Z + t f is the exact prefix at k + t.
 // orientation 0: slices y, columns x (Z_y); 1: slices x, columns y (Z_x).
 cudaError_t launch_zt(const float *vol, const unsigned char *mask, int XN, int YN, int ZN, int orientation,
-                      float *out, int rs, cudaStream_t s);
+                      float2 *out, int rs, cudaStream_t s);
 // The same for the voxel columns with y in [y0, y1) only (y0 a multiple of
 // 32), so a volume uploaded in y slabs can be prefixed slab by slab.
 cudaError_t launch_zt_rows(const float *vol, const unsigned char *mask, int XN, int YN, int ZN, int orientation,
-                           float *out, int rs, int y0, int y1, cudaStream_t s);
+                           float2 *out, int rs, int y0, int y1, cudaStream_t s);
 
 // Projection SAT: Q[p][u'][v'] of W = prj * L (L = slab path weight of the
 // view's driving axis) for n views of the list.
@@ -206,9 +208,9 @@ struct ProjArgs {
     int ngroups, G;
     int nbuf;             // staging depth (proj_staging)
     // slice-major z-prefix projector (sat mode ZPREFIX)
-    const float *zt_y, *zt_x; // [YN][ZN+1][zt_rs_y], [XN][ZN+1][zt_rs_x]
+    const float2 *zt_y, *zt_x; // (Z, f) pairs [YN][ZN+1][zt_rs_y], [XN][ZN+1][zt_rs_x]
     int zt_rs_y, zt_rs_x;
-    int t_cb, t_kb, t_kr;     // stage: [t_kr][t_cb] floats, TMA boxes of t_kb rows
+    int t_cb, t_kb, t_kr;      // stage: [t_kr][t_cb] pairs, TMA boxes of t_kb rows
     int t_nstage, t_rb, t_ep, t_gtab; // stages, consumer warps per view, z-boundary pitch, table views
     int t_zs;                         // detector rows split over t_zs CTAs
     int t_nr;                         // detector rows per consumer warp (t_nr * t_rb rows per CTA)

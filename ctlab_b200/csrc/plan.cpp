@@ -47,17 +47,18 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
     return fn;
 }
 
-// TMA map of a slice-major z-prefix array [na][ZN+1][rs] (nb valid columns):
+// TMA map of a slice-major z-prefix pair array [na][ZN+1][rs] (nb valid
+// columns; each element an 8-byte (Z, f) pair, moved as one 64-bit word):
 // boxes of CB columns x KB rows x 1 slice, zero fill outside.
-int encode_zt_map(CUtensorMap *m, float *base, int nb, int ZN, int na, int rs, int CB, int KB)
+int encode_zt_map(CUtensorMap *m, float2 *base, int nb, int ZN, int na, int rs, int CB, int KB)
 {
     PFN_cuTensorMapEncodeTiled_v12000 fn = tensor_map_encoder();
     if (!fn) return set_status(CTLAB_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
     const cuuint64_t dims[3] = {(cuuint64_t)nb, (cuuint64_t)ZN + 1, (cuuint64_t)na};
-    const cuuint64_t strides[2] = {(cuuint64_t)rs * 4, (cuuint64_t)(ZN + 1) * rs * 4};
+    const cuuint64_t strides[2] = {(cuuint64_t)rs * 8, (cuuint64_t)(ZN + 1) * rs * 8};
     const cuuint32_t box[3] = {(cuuint32_t)CB, (cuuint32_t)KB, 1};
     const cuuint32_t es[3] = {1, 1, 1};
-    const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, es,
+    const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, base, dims, strides, box, es,
                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return set_status(CTLAB_ERR_CUDA, "cuTensorMapEncodeTiled failed for a z-prefix array");
@@ -599,8 +600,14 @@ int ctlab_copy_volume_sat(ctlab_plan *plan, int orientation, void *d_out, void *
     const bool zpre = plan->sat_mode == CTLAB_SAT_ZPREFIX;
     const void *src = zpre ? (const void *)(orientation == 0 ? plan->d_zt_y : plan->d_zt_x)
                            : (orientation == 0 ? plan->d_sat_y : plan->d_sat_x);
-    CTLAB_CUDA_TRY(cudaMemcpyAsync(d_out, src, (zpre ? 4 : 8) * (size_t)planes * rows * zp, cudaMemcpyDeviceToDevice,
-                                   (cudaStream_t)stream));
+    if (zpre) {
+        // the prefixes Z of the (Z, f) pairs
+        CTLAB_CUDA_TRY(cudaMemcpy2DAsync(d_out, sizeof(float), src, sizeof(float2), sizeof(float),
+                                         (size_t)planes * rows * zp, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+    } else {
+        CTLAB_CUDA_TRY(cudaMemcpyAsync(d_out, src, 8 * (size_t)planes * rows * zp, cudaMemcpyDeviceToDevice,
+                                       (cudaStream_t)stream));
+    }
     return ok();
 }
 

@@ -2,13 +2,14 @@
 // z-prefixes (sat mode CTLAB_SAT_ZPREFIX).
 //
 // Volume data, one array per driving axis: planes j (the slices along the
-// axis) of ZN+1 rows k by nb columns c, c fastest,
+// axis) of ZN+1 rows k by nb columns c, c fastest, of (prefix, slope) pairs
 //     Z[j][k][c] = sum_{z<k} f(column c of slice j, z)   (FP64 sums, FP32),
+//     f[j][k][c] = f(column c of slice j, k),
 // i.e. Z_y[y][k][x] for y-driven views and Z_x[x][k][y] for x-driven ones.
-// For piecewise-constant voxels the z-prefix interpolated linearly in z is
-// the exact integral of the column up to kz, so the integral over an
-// axis-aligned rectangle of a slice is a weighted sum of interpolated
-// column prefixes -- the difference-of-SAT of the branchless DD method with
+// For piecewise-constant voxels Z + (kz - k) f is the exact integral of the
+// column up to kz (k = floor(kz)), so the integral over an axis-aligned
+// rectangle of a slice is a weighted sum of column prefixes, each one 64-bit
+// load and one FMA -- the difference-of-SAT of the branchless DD method with
 // the FP64 in-plane prefix replaced by its exact column differences (which
 // the 2-D FP64 SAT path also rounds to FP32 before use).
 //
@@ -29,7 +30,7 @@
 //                  width in columns).  For each of the NR+1 z boundaries e_w,
 //                      kz = Z0 + T e_w,
 //                      F(kz) = wa Za(kz) + wb Zb(kz) [+ whole columns between],
-//                  Zc(kz) the column prefix interpolated in z, and
+//                  Zc(kz) = Z + (kz - k) f of column c's pair at row k, and
 //                      acc[v] += (F(kz_{v+1}) - F(kz_v)) / (W T).
 //                  Lanes read neighbouring columns of nearly the same rows,
 //                  so the shared-memory loads are free of bank conflicts.
@@ -72,10 +73,10 @@ struct TSlice {
     int pad1;
 };
 
-__device__ __forceinline__ float lds_f32(uint32_t addr)
+__device__ __forceinline__ float2 lds_f32x2(uint32_t addr)
 {
-    float v;
-    asm("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr));
+    float2 v;
+    asm("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr));
     return v;
 }
 __device__ __forceinline__ float4 lds_f32x4(uint32_t addr)
@@ -85,27 +86,27 @@ __device__ __forceinline__ float4 lds_f32x4(uint32_t addr)
     return v;
 }
 
-// z-interpolated column prefix at the row fraction fz: rows at pa and pa + RS4
-__device__ __forceinline__ float zinterp(uint32_t pa, uint32_t RS4, float fz)
+// column prefix at the row fraction fz from the (Z, f) pair at pa
+__device__ __forceinline__ float zinterp(uint32_t pa, float fz)
 {
-    const float c0 = lds_f32(pa), c1 = lds_f32(pa + RS4);
-    return fmaf(fz, c1 - c0, c0);
+    const float2 zf = lds_f32x2(pa);
+    return fmaf(fz, zf.y, zf.x);
 }
 
-// Staged slice address of the z-prefix row holding kz, clamped to the box
-// [kz_lo, kz_hi], and the fraction of kz past that row.  The caller passes
-// kz normalised to the box, vn = (kz - kz_lo) / span with span = kz_hi -
-// kz_lo, as vn = Tn e + z0n: one saturating FMA clamps, and the
-// round-toward-zero FMA adding 2^23 leaves floor(vn span) -- the row past
-// kz_lo -- in the mantissa bits; base folds in the box origin and the 2^23
-// exponent bits.
-__device__ __forceinline__ uint32_t zrow_addr(float Tn, float e, float z0n, float span, uint32_t RS4, uint32_t base,
+// Staged slice address of the z-prefix pair of the row holding kz, clamped
+// to the box [kz_lo, kz_hi], and the fraction of kz past that row.  The
+// caller passes kz normalised to the box, vn = (kz - kz_lo) / span with
+// span = kz_hi - kz_lo, as vn = Tn e + z0n: one saturating FMA clamps, and
+// the round-toward-zero FMA adding 2^23 leaves floor(vn span) -- the row
+// past kz_lo -- in the mantissa bits; base folds in the box origin and the
+// 2^23 exponent bits (RS: bytes per staged row).
+__device__ __forceinline__ uint32_t zrow_addr(float Tn, float e, float z0n, float span, uint32_t RS, uint32_t base,
                                               float &fz)
 {
     const float vn = __saturatef(fmaf(Tn, e, z0n));
     const float rr = __fmaf_rz(vn, span, 8388608.f);
     fz = fmaf(vn, span, 8388608.f - rr);
-    return __float_as_uint(rr) * RS4 + base;
+    return __float_as_uint(rr) * RS + base;
 }
 
 // Rows of one detector column on one slice when every strip of the warp
@@ -113,9 +114,9 @@ __device__ __forceinline__ uint32_t zrow_addr(float Tn, float e, float z0n, floa
 // F(row boundary) = wa Z(a) + wb Z(b); acc[r] += (F(r + 1) - F(r)) scale.
 template <int NR>
 __device__ __forceinline__ void rows_narrow(float (&acc)[NR], const TEntry &te, int dc, uint32_t e_addr, uint32_t base,
-                                            uint32_t RS4, float Tn, float z0n, float span)
+                                            uint32_t RS, float Tn, float z0n, float span)
 {
-    const uint32_t dc4 = 4u * (uint32_t)dc;
+    const uint32_t dc8 = 8u * (uint32_t)dc;
     float prev = 0.f;
 #pragma unroll
     for (int r4 = 0; r4 <= NR; r4 += 4) {
@@ -126,10 +127,9 @@ __device__ __forceinline__ void rows_narrow(float (&acc)[NR], const TEntry &te, 
             const int r = r4 + q;
             if (r > NR) break;
             float fz;
-            const uint32_t pa = zrow_addr(Tn, ev[q], z0n, span, RS4, base, fz), pb = pa + dc4;
-            const float a0 = lds_f32(pa), a1 = lds_f32(pa + RS4);
-            const float b0 = lds_f32(pb), b1 = lds_f32(pb + RS4);
-            const float F = fmaf(te.wb, fmaf(fz, b1 - b0, b0), te.wa * fmaf(fz, a1 - a0, a0));
+            const uint32_t pa = zrow_addr(Tn, ev[q], z0n, span, RS, base, fz), pb = pa + dc8;
+            const float2 za = lds_f32x2(pa), zb = lds_f32x2(pb);
+            const float F = fmaf(te.wb, fmaf(fz, zb.y, zb.x), te.wa * fmaf(fz, za.y, za.x));
             if (r > 0) acc[r - 1] = fmaf(F - prev, te.scale, acc[r - 1]);
             prev = F;
         }
@@ -148,16 +148,16 @@ __device__ __forceinline__ float strip_weight(const TEntry &te, int i, int dc, i
 // voxel columns: one pass over the columns a .. a + M sgn(dc) per row.
 template <int NR, int M>
 __device__ __forceinline__ void rows_wide(float (&acc)[NR], const TEntry &te, int dc, uint32_t e_addr, uint32_t base,
-                                          uint32_t RS4, float Tn, float z0n, float span)
+                                          uint32_t RS, float Tn, float z0n, float span)
 {
     const int adc = dc < 0 ? -dc : dc;
-    const int step4 = dc < 0 ? -4 : 4;
+    const int step8 = dc < 0 ? -8 : 8;
     float w[M + 1];
     uint32_t off[M + 1];
 #pragma unroll
     for (int i = 0; i <= M; ++i) {
         w[i] = strip_weight(te, i, dc, adc);
-        off[i] = (uint32_t)(min(i, adc) * step4);
+        off[i] = (uint32_t)(min(i, adc) * step8);
     }
     float prev = 0.f;
 #pragma unroll
@@ -169,10 +169,10 @@ __device__ __forceinline__ void rows_wide(float (&acc)[NR], const TEntry &te, in
             const int r = r4 + q;
             if (r > NR) break;
             float fz;
-            const uint32_t pa = zrow_addr(Tn, ev[q], z0n, span, RS4, base, fz);
-            float F = w[0] * zinterp(pa, RS4, fz);
+            const uint32_t pa = zrow_addr(Tn, ev[q], z0n, span, RS, base, fz);
+            float F = w[0] * zinterp(pa, fz);
 #pragma unroll
-            for (int i = 1; i <= M; ++i) F = fmaf(w[i], zinterp(pa + off[i], RS4, fz), F);
+            for (int i = 1; i <= M; ++i) F = fmaf(w[i], zinterp(pa + off[i], fz), F);
             if (r > 0) acc[r - 1] = fmaf(F - prev, te.scale, acc[r - 1]);
             prev = F;
         }
@@ -203,9 +203,9 @@ __device__ __forceinline__ void proj_t_tile(const ProjArgs &a, const CUtensorMap
     const int vbase = bz * RB * NR; // first detector row of this CTA (rows split over CTAs)
     const int nstage = a.t_nstage;
     const int CB = a.t_cb, KB = a.t_kb, KR = a.t_kr, EP = a.t_ep, GT = a.t_gtab;
-    const int stage_floats = KR * CB;
-    float *stage0 = reinterpret_cast<float *>(smem);                          // [nstage][KR][CB]
-    float *s_e = reinterpret_cast<float *>(smem + 4 * stage_floats * nstage); // [GT][EP]
+    const int stage_elems = KR * CB;
+    float2 *stage0 = reinterpret_cast<float2 *>(smem);                        // [nstage][KR][CB] (Z, f)
+    float *s_e = reinterpret_cast<float *>(smem + 8 * stage_elems * nstage); // [GT][EP]
     auto &s_full = sh.full;
     auto &s_empty = sh.empty;
     auto &s_info = sh.info;
@@ -353,9 +353,9 @@ __device__ __forceinline__ void proj_t_tile(const ProjArgs &a, const CUtensorMap
                 kmin = fminf(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
                 kmax = fmaxf(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
             }
-            // TMA: the innermost (column) coordinate must be a multiple of 4
-            // floats (16 bytes); rows need no alignment
-            const int c_lo = cmin & ~3;
+            // TMA: the innermost (column) coordinate must be a multiple of 2
+            // pairs (16 bytes); rows need no alignment
+            const int c_lo = cmin & ~1;
             const int k_lo = max((int)kmin - 1, 0);
             const int k_top = min((int)kmax + 2, ZN + 1); // row of the last kz's upper neighbour
             const int nk = k_top - k_lo + 1;
@@ -372,11 +372,11 @@ __device__ __forceinline__ void proj_t_tile(const ProjArgs &a, const CUtensorMap
                 in.inv_span = in.kz_hi > in.kz_lo ? 1.f / (in.kz_hi - in.kz_lo) : 0.f;
                 in.pad1 = 0;
                 s_info[b] = in;
-                mbar_arrive_expect_tx(&s_full[b], (uint32_t)(nbox * KB * CB * 4));
+                mbar_arrive_expect_tx(&s_full[b], (uint32_t)(nbox * KB * CB * 8));
             }
             __syncwarp();
             if (lane < nbox)
-                tma_load_3d(stage0 + b * stage_floats + lane * KB * CB, tm, c_lo, k_lo + lane * KB, j, &s_full[b]);
+                tma_load_3d(stage0 + b * stage_elems + lane * KB * CB, tm, c_lo, k_lo + lane * KB, j, &s_full[b]);
             if (lane != 0) mbar_arrive(&s_full[b]);
             issued = j + 1;
         }
@@ -388,12 +388,12 @@ __device__ __forceinline__ void proj_t_tile(const ProjArgs &a, const CUtensorMap
     } else if (warp < NWC && s_pos_list[warp / RB] >= 0) {
         // ------------------------------ consumers -----------------------------
         const int g = warp / RB, v0l = (warp - g * RB) * NR;
-        const float *zt = xdrv ? a.zt_x : a.zt_y;
+        const float2 *zt = xdrv ? a.zt_x : a.zt_y;
         const int zrs = xdrv ? a.zt_rs_x : a.zt_rs_y;
         const float z0 = s_Z0[g];
         const uint32_t e_addr = smem_addr(s_e + g * EP + v0l); // 16-byte aligned (EP, v0l multiples of 4)
         const uint32_t stage_addr = smem_addr(stage0);
-        const uint32_t RS4 = 4u * (uint32_t)CB;
+        const uint32_t RS = 8u * (uint32_t)CB; // bytes per staged row
         // this lane's boundary rays x(q, j) = c0 + m j and 1/(C_a - S_a)
         const double ma = s_m[g][lane], ca0 = s_c0[g][lane], mb = s_m[g][lane + 1], cb0 = s_c0[g][lane + 1];
         const double ru = s_r[g][min(lane, nu - 1)], ga0 = s_ga0[g];
@@ -442,22 +442,22 @@ __device__ __forceinline__ void proj_t_tile(const ProjArgs &a, const CUtensorMap
             const bool staged = in.fits && m <= 3;
             const int2 cd = make_int2(staged ? ia - in.c_lo : ia, dc);
             if (staged) {
-                // address of row k_lo + i, column a = bits(i + 2^23) * RS4 + base (mod 2^32)
-                const uint32_t base = stage_addr + (uint32_t)b * 4u * (uint32_t)stage_floats + 4u * (uint32_t)cd.x -
-                                      0x4B000000u * RS4;
+                // address of row k_lo + i, column a = bits(i + 2^23) * RS + base (mod 2^32)
+                const uint32_t base = stage_addr + (uint32_t)b * 8u * (uint32_t)stage_elems + 8u * (uint32_t)cd.x -
+                                      0x4B000000u * RS;
                 // kz normalised to the box: (T e + z0 - kz_lo) / span
                 const float span = in.kz_hi - in.kz_lo;
                 const float Tn = te.T * in.inv_span, z0n = (z0 - in.kz_lo) * in.inv_span;
                 if (m <= 1)
-                    rows_narrow<NR>(acc, te, dc, e_addr, base, RS4, Tn, z0n, span);
+                    rows_narrow<NR>(acc, te, dc, e_addr, base, RS, Tn, z0n, span);
                 else if (m == 2)
-                    rows_wide<NR, 2>(acc, te, dc, e_addr, base, RS4, Tn, z0n, span);
+                    rows_wide<NR, 2>(acc, te, dc, e_addr, base, RS, Tn, z0n, span);
                 else
-                    rows_wide<NR, 3>(acc, te, dc, e_addr, base, RS4, Tn, z0n, span);
+                    rows_wide<NR, 3>(acc, te, dc, e_addr, base, RS, Tn, z0n, span);
             } else {
                 // block wider than a stage, or strips wider than four columns:
                 // the column prefixes from global memory
-                const float *S = zt + (long long)j * (ZN + 1) * zrs;
+                const float2 *S = zt + (long long)j * (ZN + 1) * zrs;
                 float prev = 0.f;
 #pragma unroll
                 for (int r = 0; r <= NR; ++r) {
@@ -466,7 +466,10 @@ __device__ __forceinline__ void proj_t_tile(const ProjArgs &a, const CUtensorMap
                     const int k0 = min((int)kz, ZN - 1);
                     const float fz = kz - (float)k0;
                     const int ia = cd.x + k0 * zrs;
-                    auto zc = [&](int i) { return fmaf(fz, __ldg(S + i + zrs) - __ldg(S + i), __ldg(S + i)); };
+                    auto zc = [&](int i) {
+                        const float2 zf = __ldg(S + i);
+                        return fmaf(fz, zf.y, zf.x);
+                    };
                     float F = te.wa * zc(ia) + te.wb * zc(ia + dc);
                     if (wide) {
                         const int n = dc > 1 ? dc - 1 : (dc < -1 ? -dc - 1 : 0);
@@ -597,7 +600,7 @@ __global__ void __launch_bounds__(kTMaxThreads, 1)
 
 size_t smem_bytes(const ProjTStaging &st)
 {
-    return 128 + 4 * (size_t)st.KR * st.CB * st.nstage + sizeof(float) * (size_t)st.G * st.EP;
+    return 128 + sizeof(float2) * (size_t)st.KR * st.CB * st.nstage + sizeof(float) * (size_t)st.G * st.EP;
 }
 
 template <int NR>
@@ -630,9 +633,9 @@ int t_span(const HostGeometry &g, const std::vector<const DevView *> &vs, int u0
     const int nb = vs[0]->nb;
     lo = std::min(std::max(lo, 0.0), (double)nb);
     hi = std::min(std::max(hi, 0.0), (double)nb);
-    // floor(lo) rounded down to 4 (TMA alignment) and one column of margin
-    // each side for rounding between host and device
-    const int c_lo = std::max((int)lo - 1, 0) & ~3;
+    // floor(lo) rounded down to 2 (TMA alignment of 8-byte pairs) and one
+    // column of margin each side for rounding between host and device
+    const int c_lo = std::max((int)lo - 1, 0) & ~1;
     const int c_hi = std::min((int)hi + 1, nb - 1);
     return c_hi - c_lo + 1;
 }
@@ -791,14 +794,16 @@ ProjTStaging proj_t_staging(const HostGeometry &g, int gcap, int nstage_fix, int
     ProjTStaging best;
     int best_key = -1;
     for (int G = gmax; G >= 1; --G) {
-        int CB = (t_need(g, as_views(t_groups(g, all, G), all)) + 3) & ~3;
-        // a row stride of 16 (mod 32) floats keeps lanes that read neighbouring
-        // rows off each other's banks; take it when it costs little
-        const int cb16 = CB + ((16 - CB % 32) + 32) % 32;
-        if (cb16 - CB <= 12) CB = cb16;
+        int CB = (t_need(g, as_views(t_groups(g, all, G), all)) + 1) & ~1;
+        // a row stride of a multiple of 16 pairs (128 bytes) puts every
+        // column on the same banks in every row, so lanes reading distinct
+        // columns never conflict whatever rows they read; take it when it
+        // costs little
+        const int cb16 = (CB + 15) & ~15;
+        if (cb16 - CB <= 8) CB = cb16;
         if (CB > cbmax) {
             if (G > 1) continue;
-            CB = cbmax & ~3; // G = 1: wider slices read global memory
+            CB = cbmax & ~1; // G = 1: wider slices read global memory
         }
         for (int ZS : {1, 2, 4}) {
             if (want_zs && ZS != want_zs) continue;
@@ -819,8 +824,8 @@ ProjTStaging proj_t_staging(const HostGeometry &g, int gcap, int nstage_fix, int
             const int zrows = t_zrows(g, as_views(t_groups(g, all, G), all), RB * NR, zs);
             const int nbox = (zrows + 255) / 256;
             int KB = (zrows + nbox - 1) / nbox;
-            // 128-byte aligned TMA destinations: KB * CB * 4 a multiple of 128
-            while ((KB * CB) % 32) ++KB;
+            // 128-byte aligned TMA destinations: KB * CB * 8 a multiple of 128
+            while ((KB * CB) % 16) ++KB;
             if (KB > 256) continue;
             for (int ns = kTMaxStage; ns >= 2; --ns) {
                 if (want_stage >= 2 && want_stage <= kTMaxStage && ns != want_stage) continue;

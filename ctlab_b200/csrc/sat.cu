@@ -318,13 +318,16 @@ namespace {
 
 // Slice-major z-prefixes: one CTA per 32 columns of one slice.  Each warp
 // scans 4 columns 32 rows at a time (coalesced loads along z, FP64 warp
-// scan plus a carried FP64 total), the rounded prefixes go through a padded
-// shared tile, and the CTA writes them out as rows of 32 adjacent columns.
+// scan plus a carried FP64 total); row k of a column is the pair
+// (Z[k], f[k]): the FP64 prefix of the voxels below k rounded to FP32 and the
+// voxel value itself, the exact slope of the prefix on [k, k+1] (0 at
+// k = ZN).  The pairs go through a padded shared tile and the CTA writes them
+// out as rows of 32 adjacent columns.
 __global__ void __launch_bounds__(256) zt_kernel(const float *__restrict__ vol, const unsigned char *mask, int XN,
-                                                 int ZN, int nb, int orientation, float *__restrict__ out, int rs,
+                                                 int ZN, int nb, int orientation, float2 *__restrict__ out, int rs,
                                                  int j0, int c_off)
 {
-    __shared__ float tile[32][33];
+    __shared__ float2 tile[32][33];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int j = blockIdx.y + j0, c0 = blockIdx.x * 32 + c_off;
     const float *col[4];
@@ -340,42 +343,52 @@ __global__ void __launch_bounds__(256) zt_kernel(const float *__restrict__ vol, 
         m[i] = valid ? (mask ? (mask[ci] ? 1.f : 0.f) : 1.f) : 0.f;
         carry[i] = 0.0;
     }
-    float *plane = out + (long long)j * (ZN + 1) * rs;
+    float2 *plane = out + (long long)j * (ZN + 1) * rs;
     const int cw = c0 + lane;
-    if (warp == 0 && cw < rs) plane[cw] = 0.f; // row 0
     for (int z0 = 0; z0 < ZN; z0 += 32) {
         const int z = z0 + lane;
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            double v = (z < ZN && m[i] != 0.f) ? (double)(__ldg(col[i] + z) * m[i]) : 0.0;
+            const float f = (z < ZN && m[i] != 0.f) ? __ldg(col[i] + z) * m[i] : 0.f;
+            double v = (double)f;
 #pragma unroll
             for (int d = 1; d < 32; d <<= 1) {
                 const double y = __shfl_up_sync(kFull, v, d);
                 if (lane >= d) v += y;
             }
             v += carry[i];
-            tile[lane][warp * 4 + i] = (float)v;
+            // the prefix below row z: the inclusive prefix of the lane below
+            const double below = __shfl_up_sync(kFull, v, 1);
+            tile[lane][warp * 4 + i] = make_float2((float)(lane == 0 ? carry[i] : below), f);
             carry[i] = __shfl_sync(kFull, v, 31);
         }
         __syncthreads();
         for (int rr = warp; rr < 32; rr += 8) {
-            const int k = z0 + 1 + rr;
-            if (k <= ZN && cw < rs) plane[(long long)k * rs + cw] = cw < nb ? tile[rr][lane] : 0.f;
+            const int k = z0 + rr;
+            if (k < ZN && cw < rs) plane[(long long)k * rs + cw] = cw < nb ? tile[rr][lane] : make_float2(0.f, 0.f);
         }
         __syncthreads();
+    }
+    // row ZN: the column total, slope 0
+    if (lane == 0) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int c = c0 + warp * 4 + i;
+            if (c < rs) plane[(long long)ZN * rs + c] = make_float2(c < nb ? (float)carry[i] : 0.f, 0.f);
+        }
     }
 }
 
 } // namespace
 
 cudaError_t launch_zt(const float *vol, const unsigned char *mask, int XN, int YN, int ZN, int orientation,
-                      float *out, int rs, cudaStream_t s)
+                      float2 *out, int rs, cudaStream_t s)
 {
     return launch_zt_rows(vol, mask, XN, YN, ZN, orientation, out, rs, 0, YN, s);
 }
 
 cudaError_t launch_zt_rows(const float *vol, const unsigned char *mask, int XN, int YN, int ZN, int orientation,
-                           float *out, int rs, int y0, int y1, cudaStream_t s)
+                           float2 *out, int rs, int y0, int y1, cudaStream_t s)
 {
     const int nb = orientation ? YN : XN, na = orientation ? XN : YN;
     if (rs < nb || na > 65535 || y0 < 0 || y1 > YN || y0 > y1) return cudaErrorInvalidValue;
