@@ -126,10 +126,10 @@ cudaError_t launch_volume_sat(const float *vol, const unsigned char *mask, int X
                               int chunk, cudaStream_t s);
 
 // Slice-major column z-prefixes of the masked volume for one driving axis,
-// as (prefix, slope) pairs: out[j][k][c] = (Z, f) with
-// Z = sum_{z<k} f(column c of slice j, z) (FP64 sums rounded to FP32) and
-// f = f(column c of slice j, k) (0 for k = ZN), k in [0, ZN]; row stride
-// rs >= nb pairs (pad columns zero).  Z + t f is the exact prefix at k + t.
+// as affine pieces: out[j][k][c] = (P, f) with f = f(column c of slice j, k)
+// (0 for k = ZN) and P = Z - k f, Z = sum_{z<k} f(column c of slice j, z)
+// (FP64, P rounded to FP32 once), k in [0, ZN]; row stride rs >= nb pairs
+// (pad columns zero).  P + kz f is the exact prefix at kz in [k, k+1].
 // orientation 0: slices y, columns x (Z_y); 1: slices x, columns y (Z_x).
 cudaError_t launch_zt(const float *vol, const unsigned char *mask, int XN, int YN, int ZN, int orientation,
                       float2 *out, int rs, cudaStream_t s);
@@ -137,6 +137,8 @@ cudaError_t launch_zt(const float *vol, const unsigned char *mask, int XN, int Y
 // 32), so a volume uploaded in y slabs can be prefixed slab by slab.
 cudaError_t launch_zt_rows(const float *vol, const unsigned char *mask, int XN, int YN, int ZN, int orientation,
                            float2 *out, int rs, int y0, int y1, cudaStream_t s);
+// The prefixes Z[k] = P + k f of a pair array [planes][rows][rs] into out.
+cudaError_t launch_zt_unpack(const float2 *in, float *out, int planes, int rows, int rs, cudaStream_t s);
 
 // Projection SAT: Q[p][u'][v'] of W = prj * L (L = slab path weight of the
 // view's driving axis) for n views of the list.
@@ -208,7 +210,7 @@ struct ProjArgs {
     int ngroups, G;
     int nbuf;             // staging depth (proj_staging)
     // slice-major z-prefix projector (sat mode ZPREFIX)
-    const float2 *zt_y, *zt_x; // (Z, f) pairs [YN][ZN+1][zt_rs_y], [XN][ZN+1][zt_rs_x]
+    const float2 *zt_y, *zt_x; // (P, f) pairs [YN][ZN+1][zt_rs_y], [XN][ZN+1][zt_rs_x]
     int zt_rs_y, zt_rs_x;
     int t_cb, t_kb, t_kr;      // stage: [t_kr][t_cb] pairs, TMA boxes of t_kb rows
     int t_nstage, t_rb, t_ep, t_gtab; // stages, consumer warps per view, z-boundary pitch, table views

@@ -48,7 +48,7 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 }
 
 // TMA map of a slice-major z-prefix pair array [na][ZN+1][rs] (nb valid
-// columns; each element an 8-byte (Z, f) pair, moved as one 64-bit word):
+// columns; each element an 8-byte (P, f) pair, moved as one 64-bit word):
 // boxes of CB columns x KB rows x 1 slice, zero fill outside.
 int encode_zt_map(CUtensorMap *m, float2 *base, int nb, int ZN, int na, int rs, int CB, int KB)
 {
@@ -601,9 +601,8 @@ int ctlab_copy_volume_sat(ctlab_plan *plan, int orientation, void *d_out, void *
     const void *src = zpre ? (const void *)(orientation == 0 ? plan->d_zt_y : plan->d_zt_x)
                            : (orientation == 0 ? plan->d_sat_y : plan->d_sat_x);
     if (zpre) {
-        // the prefixes Z of the (Z, f) pairs
-        CTLAB_CUDA_TRY(cudaMemcpy2DAsync(d_out, sizeof(float), src, sizeof(float2), sizeof(float),
-                                         (size_t)planes * rows * zp, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+        // the prefixes Z = P + k f of the (P, f) pairs
+        CTLAB_CUDA_TRY(launch_zt_unpack((const float2 *)src, (float *)d_out, planes, rows, zp, (cudaStream_t)stream));
     } else {
         CTLAB_CUDA_TRY(cudaMemcpyAsync(d_out, src, 8 * (size_t)planes * rows * zp, cudaMemcpyDeviceToDevice,
                                        (cudaStream_t)stream));

@@ -21,7 +21,7 @@ struct ctlab_plan {
     std::vector<int> h_list;
     bool need_y = false, need_x = false;
     void *d_sat_y = nullptr, *d_sat_x = nullptr;
-    float2 *d_zt_y = nullptr, *d_zt_x = nullptr; // slice-major (Z, f) z-prefix pairs (sat mode ZPREFIX)
+    float2 *d_zt_y = nullptr, *d_zt_x = nullptr; // slice-major (P, f) z-prefix pairs (sat mode ZPREFIX)
     int zt_rs_y = 0, zt_rs_x = 0;               // their row strides (floats)
     CUtensorMap tm_y, tm_x;                     // TMA maps of the z-prefix arrays
     ctlab::ProjTStaging tst;                    // z-prefix projector staging

@@ -2,16 +2,16 @@
 // z-prefixes (sat mode CTLAB_SAT_ZPREFIX).
 //
 // Volume data, one array per driving axis: planes j (the slices along the
-// axis) of ZN+1 rows k by nb columns c, c fastest, of (prefix, slope) pairs
-//     Z[j][k][c] = sum_{z<k} f(column c of slice j, z)   (FP64 sums, FP32),
-//     f[j][k][c] = f(column c of slice j, k),
-// i.e. Z_y[y][k][x] for y-driven views and Z_x[x][k][y] for x-driven ones.
-// For piecewise-constant voxels Z + (kz - k) f is the exact integral of the
-// column up to kz (k = floor(kz)), so the integral over an axis-aligned
-// rectangle of a slice is a weighted sum of column prefixes, each one 64-bit
-// load and one FMA -- the difference-of-SAT of the branchless DD method with
-// the FP64 in-plane prefix replaced by its exact column differences (which
-// the 2-D FP64 SAT path also rounds to FP32 before use).
+// axis) of ZN+1 rows k by nb columns c, c fastest, of pairs (P, f) with
+//     Z[j][k][c] = sum_{z<k} f(column c of slice j, z)   (FP64 sums),
+//     f = f(column c of slice j, k),  P = Z - k f   (FP64, stored FP32),
+// i.e. for y-driven views planes y, columns x, and for x-driven ones planes
+// x, columns y.  For piecewise-constant voxels P + kz f is the exact
+// integral of the column up to kz on [k, k+1], so the integral over an
+// axis-aligned rectangle of a slice is a weighted sum of column prefixes,
+// each one 64-bit load and one FMA -- the difference-of-SAT of the
+// branchless DD method with the FP64 in-plane prefix replaced by its exact
+// column differences (which the 2-D FP64 SAT path also rounds to FP32).
 //
 // One CTA owns 32 detector columns (one per lane) of a group of G views of
 // one driving axis with adjacent angles and sweeps the slices.
@@ -30,7 +30,7 @@
 //                  width in columns).  For each of the NR+1 z boundaries e_w,
 //                      kz = Z0 + T e_w,
 //                      F(kz) = wa Za(kz) + wb Zb(kz) [+ whole columns between],
-//                  Zc(kz) = Z + (kz - k) f of column c's pair at row k, and
+//                  Zc(kz) = P + kz f of column c's pair at row k, and
 //                      acc[v] += (F(kz_{v+1}) - F(kz_v)) / (W T).
 //                  Lanes read neighbouring columns of nearly the same rows,
 //                  so the shared-memory loads are free of bank conflicts.
@@ -79,6 +79,13 @@ __device__ __forceinline__ float2 lds_f32x2(uint32_t addr)
     asm("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr));
     return v;
 }
+template <int OFF>
+__device__ __forceinline__ float2 lds_f32x2_at(uint32_t addr)
+{
+    float2 v;
+    asm("ld.shared.v2.f32 {%0, %1}, [%2+%3];" : "=f"(v.x), "=f"(v.y) : "r"(addr), "n"(OFF));
+    return v;
+}
 __device__ __forceinline__ float4 lds_f32x4(uint32_t addr)
 {
     float4 v;
@@ -86,37 +93,38 @@ __device__ __forceinline__ float4 lds_f32x4(uint32_t addr)
     return v;
 }
 
-// column prefix at the row fraction fz from the (Z, f) pair at pa
-__device__ __forceinline__ float zinterp(uint32_t pa, float fz)
+// column prefix at kz from the (P, f) pair at pa
+__device__ __forceinline__ float zinterp(uint32_t pa, float kz)
 {
-    const float2 zf = lds_f32x2(pa);
-    return fmaf(fz, zf.y, zf.x);
+    const float2 pf = lds_f32x2(pa);
+    return fmaf(kz, pf.y, pf.x);
 }
 
-// Staged slice address of the z-prefix pair of the row holding kz, clamped
-// to the box [kz_lo, kz_hi], and the fraction of kz past that row.  The
-// caller passes kz normalised to the box, vn = (kz - kz_lo) / span with
-// span = kz_hi - kz_lo, as vn = Tn e + z0n: one saturating FMA clamps, and
-// the round-toward-zero FMA adding 2^23 leaves floor(vn span) -- the row
-// past kz_lo -- in the mantissa bits; base folds in the box origin and the
-// 2^23 exponent bits (RS: bytes per staged row).
-__device__ __forceinline__ uint32_t zrow_addr(float Tn, float e, float z0n, float span, uint32_t RS, uint32_t base,
-                                              float &fz)
+// Staged slice address of the z-prefix pair of the row holding kz, and kz,
+// both clamped to the box [kz_lo, kz_hi].  The caller passes kz normalised
+// to the box, vn = (kz - kz_lo) / span with span = kz_hi - kz_lo, as
+// vn = Tn e + z0n: one saturating FMA clamps, the round-toward-zero FMA
+// adding 2^23 leaves floor(vn span) -- the row past kz_lo -- in the mantissa
+// bits, and one FMA gives kz; base folds in the box origin and the 2^23
+// exponent bits (RS: bytes per staged row).
+__device__ __forceinline__ uint32_t zrow_addr(float Tn, float e, float z0n, float span, float kz_lo, uint32_t RS,
+                                              uint32_t base, float &kz)
 {
     const float vn = __saturatef(fmaf(Tn, e, z0n));
     const float rr = __fmaf_rz(vn, span, 8388608.f);
-    fz = fmaf(vn, span, 8388608.f - rr);
+    kz = fmaf(vn, span, kz_lo);
     return __float_as_uint(rr) * RS + base;
 }
 
 // Rows of one detector column on one slice when every strip of the warp
-// spans at most two voxel columns (a and b = a + dc, |dc| <= 1):
-// F(row boundary) = wa Z(a) + wb Z(b); acc[r] += (F(r + 1) - F(r)) scale.
+// spans at most two voxel columns: the lower one lo (base) and lo + 1 (the
+// next pair, an immediate offset; weight 0 when the strip lies in one
+// column).  F(row boundary) = wlo Z(lo) + whi Z(lo + 1); acc[r] += (F(r + 1)
+// - F(r)) scale.
 template <int NR>
-__device__ __forceinline__ void rows_narrow(float (&acc)[NR], const TEntry &te, int dc, uint32_t e_addr, uint32_t base,
-                                            uint32_t RS, float Tn, float z0n, float span)
+__device__ __forceinline__ void rows_narrow(float (&acc)[NR], float wlo, float whi, float scale, uint32_t e_addr,
+                                            uint32_t base, uint32_t RS, float Tn, float z0n, float span, float kz_lo)
 {
-    const uint32_t dc8 = 8u * (uint32_t)dc;
     float prev = 0.f;
 #pragma unroll
     for (int r4 = 0; r4 <= NR; r4 += 4) {
@@ -126,11 +134,11 @@ __device__ __forceinline__ void rows_narrow(float (&acc)[NR], const TEntry &te, 
         for (int q = 0; q < 4; ++q) {
             const int r = r4 + q;
             if (r > NR) break;
-            float fz;
-            const uint32_t pa = zrow_addr(Tn, ev[q], z0n, span, RS, base, fz), pb = pa + dc8;
-            const float2 za = lds_f32x2(pa), zb = lds_f32x2(pb);
-            const float F = fmaf(te.wb, fmaf(fz, zb.y, zb.x), te.wa * fmaf(fz, za.y, za.x));
-            if (r > 0) acc[r - 1] = fmaf(F - prev, te.scale, acc[r - 1]);
+            float kz;
+            const uint32_t pa = zrow_addr(Tn, ev[q], z0n, span, kz_lo, RS, base, kz);
+            const float2 za = lds_f32x2(pa), zb = lds_f32x2_at<8>(pa);
+            const float F = fmaf(whi, fmaf(kz, zb.y, zb.x), wlo * fmaf(kz, za.y, za.x));
+            if (r > 0) acc[r - 1] = fmaf(F - prev, scale, acc[r - 1]);
             prev = F;
         }
     }
@@ -148,7 +156,7 @@ __device__ __forceinline__ float strip_weight(const TEntry &te, int i, int dc, i
 // voxel columns: one pass over the columns a .. a + M sgn(dc) per row.
 template <int NR, int M>
 __device__ __forceinline__ void rows_wide(float (&acc)[NR], const TEntry &te, int dc, uint32_t e_addr, uint32_t base,
-                                          uint32_t RS, float Tn, float z0n, float span)
+                                          uint32_t RS, float Tn, float z0n, float span, float kz_lo)
 {
     const int adc = dc < 0 ? -dc : dc;
     const int step8 = dc < 0 ? -8 : 8;
@@ -168,11 +176,11 @@ __device__ __forceinline__ void rows_wide(float (&acc)[NR], const TEntry &te, in
         for (int q = 0; q < 4; ++q) {
             const int r = r4 + q;
             if (r > NR) break;
-            float fz;
-            const uint32_t pa = zrow_addr(Tn, ev[q], z0n, span, RS, base, fz);
-            float F = w[0] * zinterp(pa, fz);
+            float kz;
+            const uint32_t pa = zrow_addr(Tn, ev[q], z0n, span, kz_lo, RS, base, kz);
+            float F = w[0] * zinterp(pa, kz);
 #pragma unroll
-            for (int i = 1; i <= M; ++i) F = fmaf(w[i], zinterp(pa + off[i], fz), F);
+            for (int i = 1; i <= M; ++i) F = fmaf(w[i], zinterp(pa + off[i], kz), F);
             if (r > 0) acc[r - 1] = fmaf(F - prev, te.scale, acc[r - 1]);
             prev = F;
         }
@@ -204,7 +212,7 @@ __device__ __forceinline__ void proj_t_tile(const ProjArgs &a, const CUtensorMap
     const int nstage = a.t_nstage;
     const int CB = a.t_cb, KB = a.t_kb, KR = a.t_kr, EP = a.t_ep, GT = a.t_gtab;
     const int stage_elems = KR * CB;
-    float2 *stage0 = reinterpret_cast<float2 *>(smem);                        // [nstage][KR][CB] (Z, f)
+    float2 *stage0 = reinterpret_cast<float2 *>(smem);                        // [nstage][KR][CB] (P, f)
     float *s_e = reinterpret_cast<float *>(smem + 8 * stage_elems * nstage); // [GT][EP]
     auto &s_full = sh.full;
     auto &s_empty = sh.empty;
@@ -359,7 +367,9 @@ __device__ __forceinline__ void proj_t_tile(const ProjArgs &a, const CUtensorMap
             const int k_lo = max((int)kmin - 1, 0);
             const int k_top = min((int)kmax + 2, ZN + 1); // row of the last kz's upper neighbour
             const int nk = k_top - k_lo + 1;
-            const bool fits = CB > 0 && (cmax - c_lo + 1 <= CB) && (nk <= KR);
+            // (one column past cmax: the narrow path reads the pair right of
+            // a strip's lower column, with weight 0 where the strip ends there)
+            const bool fits = CB > 0 && (cmax - c_lo + 2 <= CB) && (nk <= KR);
             const int nbox = fits ? (nk + KB - 1) / KB : 0;
             if (lane == 0) {
                 TSlice in;
@@ -440,7 +450,9 @@ __device__ __forceinline__ void proj_t_tile(const ProjArgs &a, const CUtensorMap
             const int m = (int)__reduce_max_sync(0xffffffffu, (unsigned)adc);
             const bool wide = m > 1;
             const bool staged = in.fits && m <= 3;
-            const int2 cd = make_int2(staged ? ia - in.c_lo : ia, dc);
+            // the narrow path addresses the strip's lower column
+            const int lo = (m <= 1 && dc < 0) ? ib : ia;
+            const int2 cd = make_int2(staged ? lo - in.c_lo : ia, dc);
             if (staged) {
                 // address of row k_lo + i, column a = bits(i + 2^23) * RS + base (mod 2^32)
                 const uint32_t base = stage_addr + (uint32_t)b * 8u * (uint32_t)stage_elems + 8u * (uint32_t)cd.x -
@@ -449,11 +461,12 @@ __device__ __forceinline__ void proj_t_tile(const ProjArgs &a, const CUtensorMap
                 const float span = in.kz_hi - in.kz_lo;
                 const float Tn = te.T * in.inv_span, z0n = (z0 - in.kz_lo) * in.inv_span;
                 if (m <= 1)
-                    rows_narrow<NR>(acc, te, dc, e_addr, base, RS, Tn, z0n, span);
+                    rows_narrow<NR>(acc, dc < 0 ? te.wb : te.wa, dc < 0 ? te.wa : te.wb, te.scale, e_addr, base, RS,
+                                    Tn, z0n, span, in.kz_lo);
                 else if (m == 2)
-                    rows_wide<NR, 2>(acc, te, dc, e_addr, base, RS, Tn, z0n, span);
+                    rows_wide<NR, 2>(acc, te, dc, e_addr, base, RS, Tn, z0n, span, in.kz_lo);
                 else
-                    rows_wide<NR, 3>(acc, te, dc, e_addr, base, RS, Tn, z0n, span);
+                    rows_wide<NR, 3>(acc, te, dc, e_addr, base, RS, Tn, z0n, span, in.kz_lo);
             } else {
                 // block wider than a stage, or strips wider than four columns:
                 // the column prefixes from global memory
@@ -464,11 +477,10 @@ __device__ __forceinline__ void proj_t_tile(const ProjArgs &a, const CUtensorMap
                     float kz = fmaf(te.T, s_e[g * EP + v0l + r], z0);
                     kz = fminf(fmaxf(kz, 0.f), (float)ZN);
                     const int k0 = min((int)kz, ZN - 1);
-                    const float fz = kz - (float)k0;
                     const int ia = cd.x + k0 * zrs;
                     auto zc = [&](int i) {
-                        const float2 zf = __ldg(S + i);
-                        return fmaf(fz, zf.y, zf.x);
+                        const float2 pf = __ldg(S + i);
+                        return fmaf(kz, pf.y, pf.x);
                     };
                     float F = te.wa * zc(ia) + te.wb * zc(ia + dc);
                     if (wide) {
@@ -636,7 +648,8 @@ int t_span(const HostGeometry &g, const std::vector<const DevView *> &vs, int u0
     // floor(lo) rounded down to 2 (TMA alignment of 8-byte pairs) and one
     // column of margin each side for rounding between host and device
     const int c_lo = std::max((int)lo - 1, 0) & ~1;
-    const int c_hi = std::min((int)hi + 1, nb - 1);
+    // (+1: the kernel reads the pair right of a strip's lower column)
+    const int c_hi = std::min((int)hi + 1, nb - 1) + 1;
     return c_hi - c_lo + 1;
 }
 

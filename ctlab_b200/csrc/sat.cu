@@ -318,10 +318,11 @@ namespace {
 
 // Slice-major z-prefixes: one CTA per 32 columns of one slice.  Each warp
 // scans 4 columns 32 rows at a time (coalesced loads along z, FP64 warp
-// scan plus a carried FP64 total); row k of a column is the pair
-// (Z[k], f[k]): the FP64 prefix of the voxels below k rounded to FP32 and the
-// voxel value itself, the exact slope of the prefix on [k, k+1] (0 at
-// k = ZN).  The pairs go through a padded shared tile and the CTA writes them
+// scan plus a carried FP64 total); row k of a column is the pair (P, f):
+// f = f[k], the voxel value and exact slope of the prefix on [k, k+1] (0 at
+// k = ZN), and P = Z[k] - k f with Z[k] the FP64 prefix of the voxels below
+// k, so that P + kz f is the prefix at kz in [k, k+1] (P rounded to FP32
+// once).  The pairs go through a padded shared tile and the CTA writes them
 // out as rows of 32 adjacent columns.
 __global__ void __launch_bounds__(256) zt_kernel(const float *__restrict__ vol, const unsigned char *mask, int XN,
                                                  int ZN, int nb, int orientation, float2 *__restrict__ out, int rs,
@@ -359,7 +360,8 @@ __global__ void __launch_bounds__(256) zt_kernel(const float *__restrict__ vol, 
             v += carry[i];
             // the prefix below row z: the inclusive prefix of the lane below
             const double below = __shfl_up_sync(kFull, v, 1);
-            tile[lane][warp * 4 + i] = make_float2((float)(lane == 0 ? carry[i] : below), f);
+            const double zk = lane == 0 ? carry[i] : below;
+            tile[lane][warp * 4 + i] = make_float2((float)(zk - (double)z * (double)f), f);
             carry[i] = __shfl_sync(kFull, v, 31);
         }
         __syncthreads();
@@ -379,7 +381,27 @@ __global__ void __launch_bounds__(256) zt_kernel(const float *__restrict__ vol, 
     }
 }
 
+// Z[k] = P + k f of every pair of a z-prefix array [planes][rows][rs].
+__global__ void __launch_bounds__(256) zt_unpack_kernel(const float2 *__restrict__ in, float *__restrict__ out,
+                                                        long long n, int rows, int rs)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)((i / rs) % rows);
+        const float2 pf = in[i];
+        out[i] = fmaf((float)k, pf.y, pf.x);
+    }
+}
+
 } // namespace
+
+cudaError_t launch_zt_unpack(const float2 *in, float *out, int planes, int rows, int rs, cudaStream_t s)
+{
+    const long long n = (long long)planes * rows * rs;
+    if (n <= 0) return cudaSuccess;
+    const int grid = (int)std::min<long long>((n + 255) / 256, 148 * 16);
+    zt_unpack_kernel<<<grid, 256, 0, s>>>(in, out, n, rows, rs);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_zt(const float *vol, const unsigned char *mask, int XN, int YN, int ZN, int orientation,
                       float2 *out, int rs, cudaStream_t s)

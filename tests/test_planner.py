@@ -2,7 +2,7 @@
 proj_t_split in libctlab_b200.so) on the benchmark scans and on edge cases:
 every staging respects the kernel's limits (rows per warp a multiple of 4 up to
 32, <= 15 consumer warps, every detector row covered, shared memory within the
-per-CTA limit, 16-byte TMA rows of (Z, f) pairs) and every view lands in exactly one group.
+per-CTA limit, 16-byte TMA rows of (P, f) pairs) and every view lands in exactly one group.
 Host only: the driver is compiled against the library, no GPU needed."""
 import os
 import re
@@ -73,7 +73,7 @@ def test_stagings_respect_the_kernel_limits(driver):
         # one CTA within the SM's limit; two 8-warp CTAs within half of it each
         assert v["smem"] + 14 * 1024 <= (227 * 1024 if W == 15 else 227 * 1024 // 2 - 1024) or v["CB"] == 0, d
         if v["CB"]:
-            # 16-byte rows of 8-byte (Z, f) pairs, 128-byte aligned boxes
+            # 16-byte rows of 8-byte (P, f) pairs, 128-byte aligned boxes
             assert v["CB"] % 2 == 0 and (v["KB"] * v["CB"]) % 16 == 0 and v["KR"] % v["KB"] == 0, d
         assert v["groupsG"] <= v["G"] and v["table"] == v["ngroups"] * v["groupsG"], d
         if v["gcap"] == 1:
