@@ -10,8 +10,10 @@
 // two CTAs per SM) and loops over the views.  Per view:
 //   geometry   the brick's voxel boundaries across the view's driving axis
 //              (8 rows of 9 points) mapped through the source onto the flat
-//              detector (FP64); each column's centre ray gives the affine
-//              z -> v map, kept normalised by DNV;
+//              detector, and each column's centre ray giving the affine
+//              z -> v map (kept normalised by DNV): FP32 on offsets from the
+//              brick centre, whose projective map (an anchor) is computed in
+//              FP64 for 32 views at a time;
 //   staging    the rows [u_lo, u_hi] of the view's P that the brick's
 //              footprint covers: one 1-D bulk copy (TMA), double buffered
 //              two views ahead and completed on an mbarrier;
@@ -147,11 +149,24 @@ struct ASet {
     int nm, pad;
 };
 
-__device__ __forceinline__ double u_of(const DevView &V, double px, double py)
-{
-    const double dpx = px - V.Sx, dpy = py - V.Sy;
-    return cross2(V.Sx - V.B0x, V.Sy - V.B0y, dpx, dpy) / cross2(V.Ex, V.Ey, dpx, dpy);
-}
+// One view's geometry anchored at the brick centre c (FP64 once, stored
+// FP32).  For a point p = c + (ox, oy) dx in the plane, the detector column
+// coordinate of the ray through p is
+//     u(p) = u0 + (gx ox + gy oy) / (1 + kx ox + ky oy),   u0 = u(c),
+// (u = N/D with N, D affine in p: gx, gy = dx (grad N - u0 grad D) / D(c),
+// kx, ky = dx grad D / D(c)), and the central-ray magnification of the
+// voxel column through p is T0 / (1 + kx ox + ky oy).  The per-view work is
+// then FP32 on offsets of a few voxels (u relative to floor(u0)), exact to
+// a few 1e-7 of a detector cell.  The z -> v map of a column with
+// magnification t is V1 = Cz t, V0 = Az + Bz t (detector rows / DNV).
+struct Anchor {
+    int iu0;   // floor(u0)
+    float fu0; // u0 - floor(u0)
+    float gx, gy, kx, ky;
+    float T0, Az, Bz, Cz;
+    int xdrv;
+};
+constexpr int kAnc = 32; // anchors per chunk: one warp, one view per lane
 
 template <int ZS, int KSEG, int VPT, bool ZSKIP>
 __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel(BackArgs a, int es2, int rmax)
@@ -166,7 +181,9 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
     float *pbuf = reinterpret_cast<float *>(E2 + EB * (size_t)kCols * es2); // [2][rmax][vp]
     __shared__ __align__(8) uint64_t s_bar[2];
     __shared__ int s_ulo[2], s_rows[2];
-    __shared__ double s_u[kGeo][kB][kB + 1];
+    __shared__ float s_u[kGeo][kB][kB + 1]; // boundaries on the detector, relative to s_iu0
+    __shared__ int s_iu0[kGeo];
+    __shared__ Anchor s_anc[2][kAnc];       // chunks of view anchors, double buffered
     __shared__ float s_V0[kGeo][kCols], s_V1[kGeo][kCols];
     __shared__ int s_xdrv[kGeo];
     __shared__ int s_cov[kGeo][2]; // the view's cone meets this CTA's z range (per column half)
@@ -203,35 +220,62 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
         mbar_fence_init();
     }
 
-    // per-view geometry of view list entry l into slot l % kGeo: the brick's
-    // voxel boundaries across the driving axis on the detector (warps 0-2)
-    // and each column's z -> v map (warps 4-5)
+    // FP64 anchors of list entries chunk * kAnc .. + kAnc - 1 into
+    // s_anc[chunk & 1] (warp 3, one view per lane)
+    auto anchors = [&](int chunk) {
+        const int i = tid - 96;
+        const int l = chunk * kAnc + i;
+        if (i < 0 || i >= kAnc || l >= n) return;
+        const DevView &V = a.views[a.view_list[lb + l]];
+        const double dpx = a.x_c0 + ((double)bx0 + 3.5) * a.dx - V.Sx;
+        const double dpy = a.y_c0 + ((double)by0 + 3.5) * a.dx - V.Sy;
+        const double D0 = cross2(V.Ex, V.Ey, dpx, dpy);                     // D(c)
+        const double N0 = cross2(V.Sx - V.B0x, V.Sy - V.B0y, dpx, dpy);     // N(c)
+        const double rD = 1.0 / D0, u0 = N0 * rD;
+        const double dDx = -V.Ey, dDy = V.Ex;                    // grad D
+        const double dNx = V.B0y - V.Sy, dNy = V.Sx - V.B0x;     // grad N
+        Anchor an;
+        const double fl = floor(u0);
+        an.iu0 = (int)fl;
+        an.fu0 = (float)(u0 - fl);
+        an.gx = (float)((dNx - u0 * dDx) * a.dx * rD);
+        an.gy = (float)((dNy - u0 * dDy) * a.dx * rD);
+        an.kx = (float)(dDx * a.dx * rD);
+        an.ky = (float)(dDy * a.dx * rD);
+        // central-ray magnification cross2(B0 - S, E) / cross2(c - S, E), the
+        // denominator being -D(c); z boundary k' -> detector row v = V0 + V1 k'
+        const double zb0 = s_zb0 + V.zP;
+        const double inv_n = 1.0 / (a.dzb * a.DNV); // detector rows, normalised by DNV
+        an.T0 = (float)(-cross2(V.B0x - V.Sx, V.B0y - V.Sy, V.Ex, V.Ey) * rD);
+        an.Az = (float)((V.Sz - zb0) * inv_n);
+        an.Bz = (float)((a.z_lo - V.Sz) * inv_n);
+        an.Cz = (float)(a.dz * inv_n);
+        an.xdrv = V.xdrv;
+        s_anc[chunk & 1][i] = an;
+    };
+    // per-view geometry of view list entry l into slot l % kGeo, from its
+    // anchor: the brick's voxel boundaries across the driving axis on the
+    // detector (warps 0-2) and each column's z -> v map (warps 4-5)
     auto geometry = [&](int l) {
         if (l >= n) return;
-        const DevView &V = a.views[a.view_list[lb + l]];
+        const Anchor &an = s_anc[(l / kAnc) & 1][l % kAnc];
         const int sl = l % kGeo;
         if (tid < kB * (kB + 1)) {
+            // boundary q (voxel q - 1/2) across the driving axis, voxel row r
+            // along it, as offsets from the brick centre
             const int r = tid / (kB + 1), q = tid - r * (kB + 1);
-            double px, py;
-            if (!V.xdrv) {
-                px = a.x_c0 + ((double)(bx0 + q) - 0.5) * a.dx;
-                py = a.y_c0 + (double)(by0 + r) * a.dx;
-            } else {
-                px = a.x_c0 + (double)(bx0 + r) * a.dx;
-                py = a.y_c0 + ((double)(by0 + q) - 0.5) * a.dx;
+            const float oq = (float)q - 4.f, orr = (float)r - 3.5f;
+            const float ox = an.xdrv ? orr : oq, oy = an.xdrv ? oq : orr;
+            s_u[sl][r][q] = an.fu0 + fmaf(an.gx, ox, an.gy * oy) / fmaf(an.kx, ox, fmaf(an.ky, oy, 1.f));
+            if (tid == 0) {
+                s_xdrv[sl] = an.xdrv;
+                s_iu0[sl] = an.iu0;
             }
-            s_u[sl][r][q] = u_of(V, px, py);
-            if (tid == 0) s_xdrv[sl] = V.xdrv;
         } else if (tid >= 128 && tid < 128 + kCols) {
             const int c = tid - 128;
-            const double pcx = a.x_c0 + (double)(bx0 + (c & (kB - 1))) * a.dx;
-            const double pcy = a.y_c0 + (double)(by0 + c / kB) * a.dx;
-            const double tc = cross2(V.B0x - V.Sx, V.B0y - V.Sy, V.Ex, V.Ey) /
-                              cross2(pcx - V.Sx, pcy - V.Sy, V.Ex, V.Ey);
-            const double zb0 = s_zb0 + V.zP;
-            // z boundary k' -> detector row coordinate v = V0 + V1 k', stored / DNV
-            const double inv_n = 1.0 / (a.dzb * a.DNV); // detector rows, normalised by DNV
-            const float V1 = (float)(tc * a.dz * inv_n), V0 = (float)((V.Sz + tc * (a.z_lo - V.Sz) - zb0) * inv_n);
+            const float ox = (float)(c & (kB - 1)) - 3.5f, oy = (float)(c / kB) - 3.5f;
+            const float tc = an.T0 / fmaf(an.kx, ox, fmaf(an.ky, oy, 1.f));
+            const float V1 = an.Cz * tc, V0 = fmaf(an.Bz, tc, an.Az);
             s_V1[sl][c] = V1;
             s_V0[sl][c] = V0;
             if (ZSKIP) {
@@ -246,17 +290,32 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
             }
         }
     };
+    // the detector cells [lo, lo + rows) the brick's footprint covers in slot
+    // sl (from its corner boundaries; one cell of margin each side)
+    auto footprint = [&](int sl, int &lo, int &rows) {
+        const float c0 = s_u[sl][0][0], c1 = s_u[sl][0][kB], c2 = s_u[sl][kB - 1][0], c3 = s_u[sl][kB - 1][kB];
+        const int iu = s_iu0[sl];
+        const int fmin_i = iu + (int)floorf(fminf(fminf(c0, c1), fminf(c2, c3)));
+        const int fmax_i = iu + (int)floorf(fmaxf(fmaxf(c0, c1), fmaxf(c2, c3)));
+        lo = max(min(max(fmin_i, 0), DNU - 1) - 1, 0);
+        rows = min(min(max(fmax_i, 0), DNU - 1) + 2, DNU - 1) - lo + 1;
+    };
+    // a boundary (relative to iu) clamped to the detector [0, DNU]: its cell
+    // and the fraction of the cell below it
+    auto cell = [&](float ul, int iu, int &i, float &f) {
+        const float uc = fminf(fmaxf(ul, (float)-iu), (float)(DNU - iu));
+        i = max(min(iu + (int)floorf(uc), DNU - 1), 0);
+        f = uc - (float)(i - iu);
+    };
     // staging of list entry l into buffer l & 1 (thread 0): the rows of P the
     // brick's footprint covers, from the corner boundaries of its geometry
     auto issue = [&](int l) {
         if (tid != 0 || l >= n) return;
         const int b = l & 1, sl = l % kGeo;
-        const double u0 = s_u[sl][0][0], u1 = s_u[sl][0][kB], u2 = s_u[sl][kB - 1][0], u3 = s_u[sl][kB - 1][kB];
-        const double umin = fmin(fmax(fmin(fmin(u0, u1), fmin(u2, u3)), 0.0), (double)(DNU - 1));
-        const double umax = fmin(fmax(fmax(fmax(u0, u1), fmax(u2, u3)), 0.0), (double)(DNU - 1));
         // one row of margin each side: interior boundaries may round past
-        // the corners' range by an ulp
-        const int lo = max((int)umin - 1, 0), rows = min((int)umax + 2, DNU - 1) - lo + 1;
+        // the corners' range
+        int lo, rows;
+        footprint(sl, lo, rows);
         const bool meets = !ZSKIP || s_cov[sl][0] || s_cov[sl][1];
         const bool fits = meets && rows <= rmax;
         s_ulo[b] = lo;
@@ -275,16 +334,15 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
         if (l >= n || tid < kSet0 || tid >= kSet0 + kCols) return;
         const int c = tid - kSet0, sl = l % kGeo;
         const int ccx = c & (kB - 1), ccy = c / kB;
-        const double u0 = s_u[sl][0][0], u1 = s_u[sl][0][kB], u2 = s_u[sl][kB - 1][0], u3 = s_u[sl][kB - 1][kB];
-        const double umin = fmin(fmax(fmin(fmin(u0, u1), fmin(u2, u3)), 0.0), (double)(DNU - 1));
-        const double umax = fmin(fmax(fmax(fmax(u0, u1), fmax(u2, u3)), 0.0), (double)(DNU - 1));
-        const int lo = max((int)umin - 1, 0), rows = min((int)umax + 2, DNU - 1) - lo + 1;
-        const int xd = s_xdrv[sl];
-        const double ua = xd ? s_u[sl][ccx][ccy] : s_u[sl][ccy][ccx];
-        const double ub = xd ? s_u[sl][ccx][ccy + 1] : s_u[sl][ccy][ccx + 1];
-        const double uca = fmin(fmax(ua, 0.0), (double)DNU), ucb = fmin(fmax(ub, 0.0), (double)DNU);
-        const int ia = min((int)uca, DNU - 1), ib = min((int)ucb, DNU - 1);
-        const float fa = (float)(uca - ia), fb = (float)(ucb - ib);
+        int lo, rows;
+        footprint(sl, lo, rows);
+        const int xd = s_xdrv[sl], iu = s_iu0[sl];
+        const float ua = xd ? s_u[sl][ccx][ccy] : s_u[sl][ccy][ccx];
+        const float ub = xd ? s_u[sl][ccx][ccy + 1] : s_u[sl][ccy][ccx + 1];
+        int ia, ib;
+        float fa, fb;
+        cell(ua, iu, ia, fa);
+        cell(ub, iu, ib, fb);
         const float sg = ((ub - ua > 0) ? 1.f : -1.f) * ((s_V1[sl][c] > 0.f) ? 1.f : -1.f);
         const int dc = ib - ia;
         float wa, wb;
@@ -318,6 +376,8 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
     };
 
     __syncthreads(); // s_zb0 visible
+    anchors(0);
+    __syncthreads(); // the first chunk of anchors visible
     geometry(0);
     geometry(1);
     geometry(2);
@@ -358,12 +418,11 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
         };
         auto strip = [&]() {
             Strip st;
-            const double ua = xdrv ? s_u[ls][acx][acy] : s_u[ls][acy][acx];
-            const double ub = xdrv ? s_u[ls][acx][acy + 1] : s_u[ls][acy][acx + 1];
-            const double uca = fmin(fmax(ua, 0.0), (double)DNU), ucb = fmin(fmax(ub, 0.0), (double)DNU);
-            st.ia = min((int)uca, DNU - 1);
-            st.ib = min((int)ucb, DNU - 1);
-            const float fa = (float)(uca - st.ia), fb = (float)(ucb - st.ib);
+            const float ua = xdrv ? s_u[ls][acx][acy] : s_u[ls][acy][acx];
+            const float ub = xdrv ? s_u[ls][acx][acy + 1] : s_u[ls][acy][acx + 1];
+            float fa, fb;
+            cell(ua, s_iu0[ls], st.ia, fa);
+            cell(ub, s_iu0[ls], st.ib, fb);
             const float sgn = ((ub - ua > 0) ? 1.f : -1.f) * ((s_V1[ls][ac] > 0.f) ? 1.f : -1.f);
             const int dc = st.ib - st.ia;
             float wa, wb;
@@ -444,6 +503,8 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
 
         // ---- stage view li+2 into the buffer just consumed; geometry of li+3 ----
         issue(li + 2);
+        // the next chunk of anchors, first read kAnc - 3 views from here
+        if (li % kAnc == 0) anchors(li / kAnc + 1);
         geometry(li + 3);
         setup(li + 2);
 
