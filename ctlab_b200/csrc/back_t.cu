@@ -393,9 +393,12 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
     for (int r = 0; r < KSEG; ++r) acc[r] = 0.f;
     bool timed_out = false;
     const uint32_t E2_addr = smem_addr(E2);
-    // phase A: kAPh threads per column, each a run of vpt consecutive rows
+    // phase A: kAPh threads per column, each a run of vpt consecutive rows;
+    // a warp's lanes are 32 columns with the same run, so its table stores
+    // (column pitch es2 odd) hit distinct banks (with 8 columns x 4 runs a
+    // warp, they conflicted: 45.4 vs 42.1 ms at 512x512x256 / 984 views)
     constexpr int kAPh = ZS;
-    const int ac = tid / kAPh, aph = tid % kAPh;
+    const int ac = tid % kCols, aph = tid / kCols;
     const int acx = ac & (kB - 1), acy = ac / kB;
     const int i0 = aph * VPT; // this thread's entries i0 .. i0+VPT-1 (kAPh*VPT > DNV)
     const float nfi0 = -(float)i0;
@@ -615,8 +618,9 @@ int e_pitch_max(int DNV) { return std::max(std::max(e_pitch(DNV, 8), e_pitch(DNV
 
 // z segments per column forced by CTLAB_BACKT_ZS (4, 8, 16), or 0: chosen
 // per launch (launch_shape).  All shapes give the same results.  On the
-// B200 at 512x512x256 / 984 views: 52.1 ms (4), 57.7 ms (8), 63.0 ms (16).
-// A warp's per-view bookkeeping (loop, waits, slot addresses, phase-A
+// B200 at 512x512x256 / 984 views: 42.1 ms with 256 threads (4); with the
+// earlier phase-A lane order, 45.4 ms (4) and 52.3 ms (8).  A warp's
+// per-view bookkeeping (loop, waits, slot addresses, phase-A
 // set-up loads) is spread over the voxels of its threads' segments, 64 / 32
 // / 16 of them; the 256-thread shape still runs 16 warps per SM, as two
 // independent CTAs whose barriers do not align.
@@ -629,9 +633,6 @@ int back_t_zs()
     }();
     return zs;
 }
-// views in a fused-update launch from which the 256-thread shape is used
-constexpr int kZs4Views = 192;
-
 size_t dyn_smem(int rmax, int vp, int es2, int ebuf = 2)
 {
     return 4 * 2 * (size_t)rmax * vp + sizeof(float2) * (size_t)ebuf * kCols * es2;
@@ -759,16 +760,14 @@ cudaError_t launch_vpt(const BackArgs &a, cudaStream_t s, BackLaunchQuery *q)
 }
 
 // The launch's block shape: CTLAB_BACKT_ZS=4, 8 or 16 forces it; otherwise
-// 256 threads (two CTAs per SM), except for the fused OS-SART update over a
-// short view list (an ordered subset), whose read-modify-write epilogue runs
-// faster spread over the 512-thread shape's twice as many threads (B200,
-// 256x256x128 / 24 subsets of 30 views: 42.3 vs 44.6 ms per iteration; a plain
-// backprojection of the same 30 views takes 0.436 ms with 256 threads and
-// 0.453 ms with 512).
+// 256 threads (two CTAs per SM), the fastest at every view count measured
+// (B200: 24 ... 984 views at 512x512x256 and 256x256x128; OS-SART with 24
+// subsets of 30 views at 256x256x128, 40.8 vs 42.4 ms per iteration with
+// the fused update on 512 threads).
 cudaError_t launch_shape(const BackArgs &a, cudaStream_t s, BackLaunchQuery *q)
 {
     int zs = back_t_zs();
-    if (zs == 0) zs = (a.epilogue == BACK_SART_UPDATE && a.n < kZs4Views) ? 8 : 4;
+    if (zs == 0) zs = 4;
     if (zs == 4 && vpt_of(a.DNV, 4) == 0) zs = 8;
     if (zs == 4) return launch_vpt<4>(a, s, q);
     return zs == 16 ? launch_vpt<16>(a, s, q) : launch_vpt<8>(a, s, q);
