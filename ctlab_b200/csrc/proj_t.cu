@@ -318,19 +318,9 @@ __device__ __forceinline__ void proj_t_tile(const ProjArgs &a, const CUtensorMap
         int issued = 0;
         for (int j = 0; j < na; ++j) {
             const int b = j % nstage;
-            if (j >= nstage) {
-                bool ok = true;
-                if (lane == 0) ok = mbar_wait(&s_empty[b], (uint32_t)(((j / nstage) - 1) & 1));
-                ok = __shfl_sync(0xffffffffu, ok, 0);
-                if (!ok) {
-                    if (lane == 0) {
-                        s_abort = 1;
-                        if (a.err) atomicExch(a.err, CTLAB_ERR_TIMEOUT);
-                    }
-                    break;
-                }
-            }
             if (*(volatile int *)&s_abort) break;
+            // slice j's box first (it needs no buffer), then the wait for the
+            // stage: only the copy's issue follows the consumers' release
             const double jd = (double)j;
             int cmin = INT_MAX, cmax = INT_MIN;
             float kmin = 1e30f, kmax = -1e30f;
@@ -371,6 +361,18 @@ __device__ __forceinline__ void proj_t_tile(const ProjArgs &a, const CUtensorMap
             // a strip's lower column, with weight 0 where the strip ends there)
             const bool fits = CB > 0 && (cmax - c_lo + 2 <= CB) && (nk <= KR);
             const int nbox = fits ? (nk + KB - 1) / KB : 0;
+            if (j >= nstage) {
+                bool ok = true;
+                if (lane == 0) ok = mbar_wait(&s_empty[b], (uint32_t)(((j / nstage) - 1) & 1));
+                ok = __shfl_sync(0xffffffffu, ok, 0);
+                if (!ok) {
+                    if (lane == 0) {
+                        s_abort = 1;
+                        if (a.err) atomicExch(a.err, CTLAB_ERR_TIMEOUT);
+                    }
+                    break;
+                }
+            }
             if (lane == 0) {
                 TSlice in;
                 in.c_lo = c_lo;
