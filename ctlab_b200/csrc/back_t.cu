@@ -109,8 +109,8 @@ __device__ __forceinline__ float2 affine_piece(float e, float en, float fi, floa
 
 // Phase A run of one thread: E at rows i0 .. i0+VPT of one column from the
 // staged P rows pa, pb (and NX whole cells pm[] between them), stored as VPT
-// affine pieces at eout (nfi0 = -i0).  Every address carries i0; offsets are
-// immediates.
+// affine pieces at eout, kCols entries apart (nfi0 = -i0).  Every address
+// carries i0; offsets are immediates.
 template <int VPT, int NX>
 __device__ __forceinline__ void phase_a_run(uint32_t pa, uint32_t pb, const uint32_t (&pm)[3], const float (&wmv)[3],
                                             float wa, float wb, float nfi0, float dnv, uint32_t eout)
@@ -128,7 +128,7 @@ __device__ __forceinline__ void phase_a_run(uint32_t pa, uint32_t pb, const uint
             const float d = e - e_prev;
             float first = fmaf(nfi0, d, e_prev);
             if constexpr (j > 1) first = fmaf(-(float)(j - 1), d, first);
-            sts_f32x2_at<8 * (j - 1)>(eout, first, dnv * d);
+            sts_f32x2_at<8 * kCols * (j - 1)>(eout, first, dnv * d);
         }
         e_prev = e;
     });
@@ -177,7 +177,10 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
     // the 512- and 1024-thread shapes, single buffered in the 256-thread one,
     // which runs two CTAs per SM and separates B from the next A by a barrier
     constexpr int EB = ZS == 4 ? 1 : 2;
-    float2 *E2 = reinterpret_cast<float2 *>(smem);                       // [EB][kCols][es2] (E, dE)
+    // the piece tables, row-major: entry i of column c at [i][c], so the 16
+    // lanes of a half-warp reading 16 consecutive columns hit distinct banks
+    // whatever rows they read
+    float2 *E2 = reinterpret_cast<float2 *>(smem);                       // [EB][es2][kCols] pieces
     float *pbuf = reinterpret_cast<float *>(E2 + EB * (size_t)kCols * es2); // [2][rmax][vp]
     __shared__ __align__(8) uint64_t s_bar[2];
     __shared__ int s_ulo[2], s_rows[2];
@@ -395,8 +398,9 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
     const uint32_t E2_addr = smem_addr(E2);
     // phase A: kAPh threads per column, each a run of vpt consecutive rows;
     // a warp's lanes are 32 columns with the same run, so its table stores
-    // (column pitch es2 odd) hit distinct banks (with 8 columns x 4 runs a
-    // warp, they conflicted: 45.4 vs 42.1 ms at 512x512x256 / 984 views)
+    // (consecutive columns of one row) hit distinct banks (with 8 columns x
+    // 4 runs a warp, they conflicted: 45.4 vs 42.1 ms at 512x512x256 / 984
+    // views)
     constexpr int kAPh = ZS;
     const int ac = tid % kCols, aph = tid / kCols;
     const int acx = ac & (kB - 1), acy = ac / kB;
@@ -462,7 +466,7 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
             const float wmv[3] = {__uint_as_float(q1.w), __uint_as_float(q2.x), __uint_as_float(q2.y)};
             // the warp runs its widest column's whole-cell count, the others with weight 0
             const int nmax = (int)__reduce_max_sync(0xffffffffu, q2.z);
-            const uint32_t eout = E2_addr + 8u * (uint32_t)((eb * kCols + ac) * es2 + i0);
+            const uint32_t eout = E2_addr + 8u * (uint32_t)((eb * es2 + i0) * kCols + ac);
             switch (nmax) {
             case 0: phase_a_run<VPT, 0>(pa, pb, pm, wmv, wa, wb, nfi0, DNVf, eout); break;
             case 1: phase_a_run<VPT, 1>(pa, pb, pm, wmv, wa, wb, nfi0, DNVf, eout); break;
@@ -474,13 +478,13 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
                 const uint32_t vp4 = 4u * (uint32_t)vp;
                 const uint32_t sbase = smem_addr(pbuf + (size_t)b * rmax * vp) + 4u * (uint32_t)i0;
                 auto row = [&](int u) { return sbase + (uint32_t)min(max(u - ulo, 0), rows - 1) * vp4; };
-                float2 *Ec = E + ac * es2;
+                float2 *Ec = E + ac;
                 float e = 0.f;
                 for (int j = 0; j <= VPT; ++j) {
                     const uint32_t o = 4u * (uint32_t)j;
                     float en = fmaf(st.wb, lds_f32(row(st.ib) + o), st.wa * lds_f32(row(st.ia) + o));
                     for (int m = 0; m < st.nm; ++m) en = fmaf(st.wm, lds_f32(row(st.first + m) + o), en);
-                    if (j > 0) Ec[i0 + j - 1] = affine_piece(e, en, (float)(i0 + j - 1), DNVf);
+                    if (j > 0) Ec[(i0 + j - 1) * kCols] = affine_piece(e, en, (float)(i0 + j - 1), DNVf);
                     e = en;
                 }
             }
@@ -489,7 +493,7 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
             // footprint wider than a stage: P from global memory
             const Strip st = strip();
             const float *Pg = a.pv + (long long)(lb + li) * DNU * vp;
-            float2 *Ec = E + ac * es2;
+            float2 *Ec = E + ac;
             auto eval = [&](int i) {
                 float e = fmaf(st.wb, __ldg(Pg + (size_t)st.ib * vp + i), st.wa * __ldg(Pg + (size_t)st.ia * vp + i));
                 for (int m = 0; m < st.nm; ++m) e = fmaf(st.wm, __ldg(Pg + (size_t)(st.first + m) * vp + i), e);
@@ -498,7 +502,7 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
             float e = eval(i0);
             for (int j = 0; j < VPT; ++j) {
                 const float en = eval(i0 + j + 1);
-                Ec[i0 + j] = affine_piece(e, en, (float)(i0 + j), DNVf);
+                Ec[(i0 + j) * kCols] = affine_piece(e, en, (float)(i0 + j), DNVf);
                 e = en;
             }
         }
@@ -514,15 +518,15 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
         // ---- phase B: voxels ----
         if (in_vol && !timed_out && (!ZSKIP || rows >= 0)) {
             const float V0 = s_V0[ls][col], V1 = s_V1[ls][col];
-            // address of (E, dE)_c[i] = bits(i + 2^23) * 8 + base (mod 2^32)
-            const uint32_t base = E2_addr + 8u * (uint32_t)(eb * kCols * es2 + col * es2) - 8u * 0x4B000000u;
+            // address of piece i of this column = bits(i + 2^23) * 8 kCols + base (mod 2^32)
+            const uint32_t base = E2_addr + 8u * (uint32_t)(eb * kCols * es2 + col) - 8u * kCols * 0x4B000000u;
             const float vb0 = fmaf(V1, (float)k0, V0);
             float prev = 0.f;
 #pragma unroll
             for (int r = 0; r <= KSEG; ++r) {
                 const float vn = __saturatef(fmaf(V1, (float)r, vb0));
                 const float rr = __fmaf_rz(vn, DNVf, 8388608.f); // 2^23 + floor(DNV vn)
-                const float2 pc = lds_f32x2(__float_as_uint(rr) * 8u + base);
+                const float2 pc = lds_f32x2(__float_as_uint(rr) * (8u * kCols) + base);
                 const float ev = fmaf(vn, pc.y, pc.x); // E_c(DNV vn)
                 if (r > 0) acc[r - 1] += ev - prev;
                 prev = ev;
@@ -703,7 +707,7 @@ struct BackLaunchQuery {
 template <int ZS, int KSEG, int VPT, bool ZSKIP>
 cudaError_t launch_k(const BackArgs &a, cudaStream_t s, BackLaunchQuery *q)
 {
-    const int es2 = e_pitch(a.DNV, ZS); // (E, dE) pairs per column, odd pitch
+    const int es2 = e_pitch(a.DNV, ZS); // pieces per column
     const size_t sm = dyn_smem(a.rmax, a.vp, es2, ZS == 4 ? 1 : 2);
     auto kern = dd3_back_t_kernel<ZS, KSEG, VPT, ZSKIP>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);

@@ -36,6 +36,7 @@ using namespace ctlab;
 // the kernel parameters); launches of different row counts run side by side.
 struct BatchLaunch {
     int nr = 0;             // detector rows per consumer warp
+    int threads = 0;        // CTA size: 512, or 256 for stagings of 8-warp CTAs (two per SM)
     std::vector<int> cases; // plan indices; work items name positions here
     int first = 0;          // first work item (d_items)
     int count = 0;          // work items
@@ -295,7 +296,9 @@ int ctlab_batch_create(ctlab_plan *const *plans, int n, ctlab_batch **out)
     DeviceGuard dg(dev);
     // work items: per item the slices of the driving axis times the views of
     // its group times the detector rows of its block.  Cases go to launches
-    // by rows per warp (in chunks of kProjBatchMaxCases); items longest first
+    // by rows per warp and CTA size (in chunks of kProjBatchMaxCases): a case
+    // whose staging plans 8-warp CTAs runs two per SM, as its own launches
+    // do, not one 16-warp CTA per SM with half the warps idle; items longest first
     // within a launch, the launch with the most work first.
     std::vector<std::vector<int4>> case_items(n);
     std::vector<std::vector<double>> case_cost(n);
@@ -312,13 +315,15 @@ int ctlab_batch_create(ctlab_plan *const *plans, int n, ctlab_batch **out)
                     case_items[i].push_back(make_int4(0, bx, gy, bz));
                     case_cost[i].push_back((double)na * c.a.G * std::min(rows, p->g.DNV - bz * rows));
                 }
+        const int threads = p->tst.W <= 7 ? 256 : 512;
         BatchLaunch *L = nullptr;
         for (BatchLaunch &l : b->launches)
-            if (l.nr == c.a.t_nr && (int)l.cases.size() < kProjBatchMaxCases) L = &l;
+            if (l.nr == c.a.t_nr && l.threads == threads && (int)l.cases.size() < kProjBatchMaxCases) L = &l;
         if (!L) {
             b->launches.emplace_back();
             L = &b->launches.back();
             L->nr = c.a.t_nr;
+            L->threads = threads;
         }
         L->cases.push_back(i);
         L->smem = std::max(L->smem, proj_t_smem_bytes(p->tst));
@@ -409,8 +414,8 @@ static int batch_enqueue(ctlab_batch *b, const float *const *d_vols, const unsig
         const BatchLaunch &l = b->launches[k];
         cudaStream_t sk = k == 0 ? s : b->side[k - 1];
         if (k > 0) CTLAB_CUDA_TRY(cudaStreamWaitEvent(sk, b->fork, 0));
-        CTLAB_CUDA_TRY(launch_proj_t_batch(l.nr, *l.params, b->d_items + l.first, l.count, b->d_counter + k, l.smem,
-                                           b->grid, sk));
+        CTLAB_CUDA_TRY(launch_proj_t_batch(l.nr, l.threads, *l.params, b->d_items + l.first, l.count,
+                                           b->d_counter + k, l.smem, b->grid * (l.threads == 256 ? 2 : 1), sk));
         if (k > 0) CTLAB_CUDA_TRY(cudaEventRecord(b->join[k - 1], sk));
     }
     for (int k = 1; k < nl; ++k) CTLAB_CUDA_TRY(cudaStreamWaitEvent(s, b->join[k - 1], 0));

@@ -268,9 +268,10 @@ struct ProjBatchParams {
 void proj_t_split(const ProjTStaging &st, int G, int &nr, int &rb);
 // Runs work items (case, detector tile, view group, row block) of up to
 // kProjBatchMaxCases cases whose launches have nr rows per consumer warp, on
-// a persistent grid; *d_counter must be 0 (stream-ordered).
-cudaError_t launch_proj_t_batch(int nr, const ProjBatchParams &cases, const int4 *d_items, int nitems, int *d_counter,
-                                size_t smem, int grid, cudaStream_t s);
+// a persistent grid of CTAs of `threads` threads (512, or 256 for cases
+// staged for 8-warp CTAs, two per SM); *d_counter must be 0 (stream-ordered).
+cudaError_t launch_proj_t_batch(int nr, int threads, const ProjBatchParams &cases, const int4 *d_items, int nitems,
+                                int *d_counter, size_t smem, int grid, cudaStream_t s);
 ProjGroups proj_t_make_groups(const HostGeometry &g, const std::vector<int> &list, const ProjTStaging &st);
 cudaError_t launch_proj_t(const ProjArgs &a, const ProjTStaging &st, const CUtensorMap &tmy, const CUtensorMap &tmx,
                           cudaStream_t s, int *launches);

@@ -761,28 +761,29 @@ size_t proj_t_smem_bytes(const ProjTStaging &st) { return smem_bytes(st); }
 
 template <int NR>
 cudaError_t launch_batch_nr(const ProjBatchParams &cases, const int4 *d_items, int nitems, int *d_counter, size_t smem,
-                            int grid, cudaStream_t s)
+                            int grid, int threads, cudaStream_t s)
 {
     auto kern = dd3_proj_t_batch_kernel<NR>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<grid, kTMaxThreads, smem, s>>>(cases, d_items, nitems, d_counter);
+    kern<<<grid, threads, smem, s>>>(cases, d_items, nitems, d_counter);
     return cudaGetLastError();
 }
 
-cudaError_t launch_proj_t_batch(int nr, const ProjBatchParams &cases, const int4 *d_items, int nitems, int *d_counter,
-                                size_t smem, int grid, cudaStream_t s)
+cudaError_t launch_proj_t_batch(int nr, int threads, const ProjBatchParams &cases, const int4 *d_items, int nitems,
+                                int *d_counter, size_t smem, int grid, cudaStream_t s)
 {
     if (nitems <= 0) return cudaSuccess;
+    if (threads != kTMaxThreads && threads != kTMaxThreads / 2) return cudaErrorInvalidValue;
     switch (nr) {
-    case 4: return launch_batch_nr<4>(cases, d_items, nitems, d_counter, smem, grid, s);
-    case 8: return launch_batch_nr<8>(cases, d_items, nitems, d_counter, smem, grid, s);
-    case 12: return launch_batch_nr<12>(cases, d_items, nitems, d_counter, smem, grid, s);
-    case 16: return launch_batch_nr<16>(cases, d_items, nitems, d_counter, smem, grid, s);
-    case 20: return launch_batch_nr<20>(cases, d_items, nitems, d_counter, smem, grid, s);
-    case 24: return launch_batch_nr<24>(cases, d_items, nitems, d_counter, smem, grid, s);
-    case 28: return launch_batch_nr<28>(cases, d_items, nitems, d_counter, smem, grid, s);
-    case 32: return launch_batch_nr<32>(cases, d_items, nitems, d_counter, smem, grid, s);
+    case 4: return launch_batch_nr<4>(cases, d_items, nitems, d_counter, smem, grid, threads, s);
+    case 8: return launch_batch_nr<8>(cases, d_items, nitems, d_counter, smem, grid, threads, s);
+    case 12: return launch_batch_nr<12>(cases, d_items, nitems, d_counter, smem, grid, threads, s);
+    case 16: return launch_batch_nr<16>(cases, d_items, nitems, d_counter, smem, grid, threads, s);
+    case 20: return launch_batch_nr<20>(cases, d_items, nitems, d_counter, smem, grid, threads, s);
+    case 24: return launch_batch_nr<24>(cases, d_items, nitems, d_counter, smem, grid, threads, s);
+    case 28: return launch_batch_nr<28>(cases, d_items, nitems, d_counter, smem, grid, threads, s);
+    case 32: return launch_batch_nr<32>(cases, d_items, nitems, d_counter, smem, grid, threads, s);
     default: return cudaErrorInvalidValue;
     }
 }
