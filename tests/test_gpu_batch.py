@@ -33,10 +33,20 @@ def uneven_scans():
               dx=1.0, dz=1.0)]
 
 
-def test_batched_projection_equals_per_scan_projection(torch_cuda):
+@pytest.mark.parametrize("warps", [None, "7", "mixed"])
+def test_batched_projection_equals_per_scan_projection(torch_cuda, warps, monkeypatch):
+    """Every case staged for 16-warp CTAs (the default), for 8-warp CTAs (CTLAB_PROJT_WARPS=7:
+    the batch runs them in 256-thread CTAs, two per SM), or both kinds in one batch."""
     torch = torch_cuda
     geoms = uneven_scans()
-    plans = [cb.Plan(g) for g in geoms]
+    plans = []
+    for i, g in enumerate(geoms):
+        if warps == "7" or (warps == "mixed" and i % 2):
+            monkeypatch.setenv("CTLAB_PROJT_WARPS", "7")
+        else:
+            monkeypatch.delenv("CTLAB_PROJT_WARPS", raising=False)
+        plans.append(cb.Plan(g))
+    monkeypatch.delenv("CTLAB_PROJT_WARPS", raising=False)
     vols, refs = [], []
     for i, (g, p) in enumerate(zip(geoms, plans)):
         hx, hy, hz = G.half_extents(g)
