@@ -13,7 +13,9 @@
 //                   M128 x N x K16 MMA per (tap, 16 channels) with both
 //                   operands in shared memory and the FP32 accumulator in
 //                   tensor memory; the CTA keeps the layer's weights in
-//                   shared memory and loops over tiles.  Epilogues: bias +
+//                   shared memory and loops over tiles, halo and
+//                   accumulator double buffered (a tile's MMAs overlap the
+//                   previous tile's epilogue).  Epilogues: bias +
 //                   ReLU, mask by an activation's sign (the data gradient =
 //                   the same convolution with the weights flipped in space
 //                   and transposed in channels), bias + centre channel in
@@ -40,7 +42,8 @@ typedef __nv_bfloat16 bf16;
 
 constexpr int kTH = 8, kTW = 16;               // output tile of a CTA: 8 rows x 16 columns
 constexpr int kHH = kTH + 2, kHW = kTW + 2;    // input halo tile
-constexpr int kCT = 128;                       // 4 warps, two tile rows each
+constexpr int kCT = 128;                       // 4 warps, two tile rows each (weight gradient)
+constexpr int kCTC = 256;                      // convolution CTA: 8 warps
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
 {
@@ -144,21 +147,25 @@ __device__ int g_cnn_err; // a convolution's MMA wait ran out (read by ctlab_cnn
 // the input halo shifted by one column each, [dx][chunk][10 rows x 16]: the
 // A operand of tap (dy, dx) is then the 128 consecutive rows of copy dx from
 // row dy, a plain descriptor.  Thread 0 issues the 9 * CI/16 MMAs and
-// commits them to an mbarrier; the 4 warps read their 32 TMEM lanes (one
-// output pixel each, CO channels) and run the epilogue.  The global loads of
-// the next tile's halo are issued before the wait for this tile's MMAs.
+// commits them to an mbarrier.  Halo copies and TMEM accumulators are double
+// buffered, so the MMAs of tile t run while the 8 warps load tile t+1's halo
+// and run tile t-1's epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31
+// (one output pixel each) and half w / 4 of the output channels.
 template <int CI, int CO>
-__global__ void __launch_bounds__(kCT, 1) conv3x3_kernel(ConvArgs a)
+__global__ void __launch_bounds__(kCTC, 1) conv3x3_kernel(ConvArgs a)
 {
     constexpr int NCH = CI / 8;                 // 16-byte chunks per input pixel
-    constexpr int TCOLS = CO < 32 ? 32 : CO;    // TMEM columns (a power of 2 >= 32)
+    constexpr int TCOLS = CO < 32 ? 32 : CO;    // TMEM columns of one accumulator (a power of 2 >= 32)
     constexpr uint32_t kPlane = kShift * 16;    // bytes of one chunk plane of a shifted tile
+    constexpr uint32_t kHaloBytes = 3 * NCH * kPlane; // the three shifted copies of one tile
     constexpr uint32_t kIdesc = umma_idesc_bf16_m128<CO>();
-    constexpr int kHalo = kHH * kHW * NCH, kPer = (kHalo + kCT - 1) / kCT; // halo chunks, per thread
+    constexpr int kHalo = kHH * kHW * NCH, kPer = (kHalo + kCTC - 1) / kCTC; // halo chunks, per thread
+    constexpr int kEH = CO >= 32 ? 2 : 1;       // epilogue channel halves (warps 4-7 take the second)
+    constexpr int kECH = CO / kEH;              // channels per epilogue thread
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char *s_w = smem;                          // [9][NCH][CO] chunks
-    unsigned char *s_a = smem + 9 * NCH * CO * 16;      // [3][NCH][kShift] chunks
-    __shared__ __align__(8) uint64_t s_bar;
+    unsigned char *s_a = smem + 9 * NCH * CO * 16;      // [2][3][NCH][kShift] chunks
+    __shared__ __align__(8) uint64_t s_bar[2];
     __shared__ uint32_t s_tmem;
     __shared__ float s_bias[CO];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -166,16 +173,16 @@ __global__ void __launch_bounds__(kCT, 1) conv3x3_kernel(ConvArgs a)
 
     // the layer's weights, 12 loads in flight per thread
     constexpr int kWChunks = CO * 9 * NCH;
-    for (int i0 = 0; i0 < kWChunks; i0 += 12 * kCT) {
+    for (int i0 = 0; i0 < kWChunks; i0 += 12 * kCTC) {
         uint4 v[12];
 #pragma unroll
         for (int u = 0; u < 12; ++u) {
-            const int i = i0 + u * kCT + tid;
+            const int i = i0 + u * kCTC + tid;
             if (i < kWChunks) v[u] = *reinterpret_cast<const uint4 *>(a.w + (size_t)(i / NCH) * CI + (i % NCH) * 8);
         }
 #pragma unroll
         for (int u = 0; u < 12; ++u) {
-            const int i = i0 + u * kCT + tid;
+            const int i = i0 + u * kCTC + tid;
             if (i < kWChunks) {
                 const int kc = i % NCH, rt = i / NCH; // rt = co*9 + tap
                 const int co = rt / 9, t = rt - co * 9;
@@ -186,11 +193,12 @@ __global__ void __launch_bounds__(kCT, 1) conv3x3_kernel(ConvArgs a)
     __syncwarp(); // the .sync.aligned tcgen05 instructions need converged warps
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&s_tmem)),
-                     "r"(TCOLS));
+                     "r"(2 * TCOLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
     }
     if (tid == 0) {
-        mbar_init(&s_bar, 1);
+        mbar_init(&s_bar[0], 1);
+        mbar_init(&s_bar[1], 1);
         mbar_fence_init();
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); // weights visible to the tensor cores
@@ -209,7 +217,7 @@ __global__ void __launch_bounds__(kCT, 1) conv3x3_kernel(ConvArgs a)
         const int y0 = (tr / tiles_x) * kTH, x0 = (tr % tiles_x) * kTW;
 #pragma unroll
         for (int u = 0; u < kPer; ++u) {
-            const int i = u * kCT + tid;
+            const int i = u * kCTC + tid;
             const int q = i % (kHH * kHW), kc = i / (kHH * kHW);
             const int row = q / kHW, col = q - row * kHW;
             const int y = y0 - 1 + row, x = x0 - 1 + col;
@@ -218,11 +226,13 @@ __global__ void __launch_bounds__(kCT, 1) conv3x3_kernel(ConvArgs a)
                 hv[u] = *reinterpret_cast<const uint4 *>(a.in + (((size_t)b * a.H + y) * a.W + x) * CI + kc * 8);
         }
     };
-    // registers -> the three column-shifted tiles (halo column col -> column col - dx of copy dx)
-    auto store_halo = [&]() {
+    // registers -> the three column-shifted tiles of buffer hb (halo column
+    // col -> column col - dx of copy dx)
+    auto store_halo = [&](int hb) {
+        unsigned char *dst = s_a + (size_t)hb * kHaloBytes;
 #pragma unroll
         for (int u = 0; u < kPer; ++u) {
-            const int i = u * kCT + tid;
+            const int i = u * kCTC + tid;
             const int q = i % (kHH * kHW), kc = i / (kHH * kHW);
             const int row = q / kHW, col = q - row * kHW;
             if (i < kHalo) {
@@ -230,7 +240,7 @@ __global__ void __launch_bounds__(kCT, 1) conv3x3_kernel(ConvArgs a)
                 for (int dx = 0; dx < 3; ++dx) {
                     const int c = col - dx;
                     if (c >= 0 && c < kTW)
-                        *reinterpret_cast<uint4 *>(s_a + (size_t)(dx * NCH + kc) * kPlane + (size_t)(row * kTW + c) * 16) =
+                        *reinterpret_cast<uint4 *>(dst + (size_t)(dx * NCH + kc) * kPlane + (size_t)(row * kTW + c) * 16) =
                             hv[u];
                 }
             }
@@ -238,101 +248,135 @@ __global__ void __launch_bounds__(kCT, 1) conv3x3_kernel(ConvArgs a)
         // generic-proxy stores visible to the tensor cores (async proxy)
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     };
-
-    uint32_t phase = 0;
-    bool ok = true;
-    load_halo(blockIdx.x);
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    // tile's MMAs (thread 0): A from halo buffer hb, accumulator hb, committed to s_bar[hb]
+    auto issue_mma = [&](int hb) {
+        if (tid != 0) return;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t a_hb = a_addr + (uint32_t)hb * kHaloBytes;
+#pragma unroll 1
+        for (int t = 0; t < 9; ++t) {
+            const int dy = t / 3, dx = t - dy * 3;
+#pragma unroll
+            for (int kk = 0; kk < CI / 16; ++kk) {
+                const uint64_t ad = umma_desc(a_hb + (uint32_t)(dx * NCH + 2 * kk) * kPlane + (uint32_t)(dy * kTW) * 16,
+                                              kPlane, 128);
+                const uint64_t bd = umma_desc(w_addr + (uint32_t)((t * NCH + 2 * kk) * CO) * 16, CO * 16, 128);
+                umma_bf16(tmem + (uint32_t)(hb * TCOLS), ad, bd, kIdesc, (t | kk) != 0);
+            }
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_addr(&s_bar[hb]))
+                     : "memory");
+    };
+    // epilogue of `tile` from accumulator ab: accumulator row m = 32 (warp % 4)
+    // + lane is output pixel (m / 16, m % 16); this warp's channel half
+    auto epilogue = [&](int tile, int ab, bool valid) {
+        const int half = warp >> 2;
+        if (half >= kEH) return; // warp-uniform
         const int b = tile / (tiles_y * tiles_x), tr = tile % (tiles_y * tiles_x);
         const int y0 = (tr / tiles_x) * kTH, x0 = (tr % tiles_x) * kTW;
-        store_halo();
-        __syncthreads();
-        if (tid == 0) {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll 1
-            for (int t = 0; t < 9; ++t) {
-                const int dy = t / 3, dx = t - dy * 3;
+        uint32_t v[kECH];
 #pragma unroll
-                for (int kk = 0; kk < CI / 16; ++kk) {
-                    const uint64_t ad = umma_desc(a_addr + (uint32_t)(dx * NCH + 2 * kk) * kPlane + (uint32_t)(dy * kTW) * 16,
-                                                  kPlane, 128);
-                    const uint64_t bd = umma_desc(w_addr + (uint32_t)((t * NCH + 2 * kk) * CO) * 16, CO * 16, 128);
-                    umma_bf16(tmem, ad, bd, kIdesc, (t | kk) != 0);
-                }
-            }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             smem_addr(&s_bar))
-                         : "memory");
-        }
-        // the next tile's halo loads are in flight while the MMAs run
-        load_halo(tile + gridDim.x);
-        const bool waited = mbar_wait(&s_bar, phase);
-        __syncwarp();
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-
-        // accumulator row m = 32 warp + lane: output pixel (m / 16, m % 16)
-        uint32_t v[CO];
-#pragma unroll
-        for (int j = 0; j < CO / 16; ++j) {
+        for (int j = 0; j < kECH / 16; ++j) {
             uint32_t r16[16];
-            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(j * 16), r16);
+            tmem_ld16(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(ab * TCOLS + half * kECH + j * 16), r16);
 #pragma unroll
             for (int e = 0; e < 16; ++e) v[j * 16 + e] = r16[e];
         }
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        const int m = warp * 32 + lane;
+        const int m = (warp & 3) * 32 + lane;
         const int y = y0 + m / kTW, x = x0 + m % kTW;
-        if (waited && y < a.H && x < a.W) {
-            const size_t pix = ((size_t)b * a.H + y) * a.W + x;
-            if (a.epi == CTLAB_CNN_EPI_RESIDUAL) {
-                a.out_f32[pix] = __uint_as_float(v[0]) + s_bias[0] + a.center[pix];
-            } else {
-                uint4 mk[CO / 8];
-                if (a.epi == CTLAB_CNN_EPI_MASK) {
+        if (!valid || y >= a.H || x >= a.W) return;
+        const size_t pix = ((size_t)b * a.H + y) * a.W + x;
+        if (a.epi == CTLAB_CNN_EPI_RESIDUAL) {
+            if (half == 0) a.out_f32[pix] = __uint_as_float(v[0]) + s_bias[0] + a.center[pix];
+            return;
+        }
+        const int c0 = half * kECH;
+        uint4 mk[kECH / 8];
+        if (a.epi == CTLAB_CNN_EPI_MASK) {
 #pragma unroll
-                    for (int c8 = 0; c8 < CO / 8; ++c8) mk[c8] = *reinterpret_cast<const uint4 *>(a.mask + pix * CO + c8 * 8);
+            for (int c8 = 0; c8 < kECH / 8; ++c8)
+                mk[c8] = *reinterpret_cast<const uint4 *>(a.mask + pix * CO + c0 + c8 * 8);
+        }
+#pragma unroll
+        for (int c8 = 0; c8 < kECH / 8; ++c8) {
+            float f[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) f[e] = __uint_as_float(v[c8 * 8 + e]);
+            if (a.epi == CTLAB_CNN_EPI_RELU) {
+#pragma unroll
+                for (int e = 0; e < 8; ++e) f[e] = fmaxf(f[e] + s_bias[c0 + c8 * 8 + e], 0.f);
+            } else if (a.epi == CTLAB_CNN_EPI_MASK) {
+                const __nv_bfloat16 *mb = reinterpret_cast<const __nv_bfloat16 *>(&mk[c8]);
+#pragma unroll
+                for (int e = 0; e < 8; ++e)
+                    if (!(__bfloat162float(mb[e]) > 0.f)) f[e] = 0.f;
+            }
+            uint4 o;
+            __nv_bfloat162 *ob = reinterpret_cast<__nv_bfloat162 *>(&o);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) ob[e] = __floats2bfloat162_rn(f[2 * e], f[2 * e + 1]);
+            *reinterpret_cast<uint4 *>(a.out + pix * CO + c0 + c8 * 8) = o;
+        }
+    };
+
+    // Iteration it (tile `tile`): halo into buffer it & 1 (its previous
+    // reader, the MMAs of iteration it - 2, completed: every thread waited
+    // for them in iteration it - 1), issue the tile's MMAs, load the next
+    // tile's halo, then wait for the previous tile's MMAs and run its
+    // epilogue while this tile's MMAs run.  Accumulator it & 1 was last read
+    // by the epilogue of iteration it - 2, finished before this iteration's
+    // barrier.  Any wait that runs out stops the whole CTA (no further halo
+    // stores or MMAs) after bounded waits for the MMAs in flight, so that
+    // tensor memory is not freed under them; the launch's output is invalid
+    // once g_cnn_err is set.
+    bool ok = true;
+    int it = 0, prev_tile = -1;
+    load_halo(blockIdx.x);
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+        const int hb = it & 1;
+        store_halo(hb);
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        issue_mma(hb);
+        load_halo(tile + gridDim.x);
+        if (it >= 1) {
+            const bool waited = mbar_wait(&s_bar[hb ^ 1], (uint32_t)(((it - 1) >> 1) & 1));
+            __syncwarp();
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            epilogue(prev_tile, hb ^ 1, waited);
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            if (__syncthreads_or(!waited)) {
+                if (tid == 0) {
+                    (void)mbar_wait(&s_bar[hb], (uint32_t)((it >> 1) & 1));
+                    (void)mbar_wait(&s_bar[hb ^ 1], (uint32_t)(((it - 1) >> 1) & 1));
                 }
-#pragma unroll
-                for (int c8 = 0; c8 < CO / 8; ++c8) {
-                    float f[8];
-#pragma unroll
-                    for (int e = 0; e < 8; ++e) f[e] = __uint_as_float(v[c8 * 8 + e]);
-                    if (a.epi == CTLAB_CNN_EPI_RELU) {
-#pragma unroll
-                        for (int e = 0; e < 8; ++e) f[e] = fmaxf(f[e] + s_bias[c8 * 8 + e], 0.f);
-                    } else if (a.epi == CTLAB_CNN_EPI_MASK) {
-                        const __nv_bfloat16 *mb = reinterpret_cast<const __nv_bfloat16 *>(&mk[c8]);
-#pragma unroll
-                        for (int e = 0; e < 8; ++e)
-                            if (!(__bfloat162float(mb[e]) > 0.f)) f[e] = 0.f;
-                    }
-                    uint4 o;
-                    __nv_bfloat162 *ob = reinterpret_cast<__nv_bfloat162 *>(&o);
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) ob[e] = __floats2bfloat162_rn(f[2 * e], f[2 * e + 1]);
-                    *reinterpret_cast<uint4 *>(a.out + pix * CO + c8 * 8) = o;
-                }
+                __syncthreads();
+                ok = false;
+                break;
             }
         }
-        // TMEM and the shifted tiles are free for the next tile -- unless any
-        // thread's wait ran out: then the whole CTA stops (no further halo
-        // stores or MMAs) after one more bounded wait for the MMAs in flight,
-        // so that tensor memory is not freed under them.  The launch's output
-        // is invalid once g_cnn_err is set.
+        prev_tile = tile;
+    }
+    if (ok && it >= 1) {
+        const int pb = (it - 1) & 1;
+        const bool waited = mbar_wait(&s_bar[pb], (uint32_t)(((it - 1) >> 1) & 1));
+        __syncwarp();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        epilogue(prev_tile, pb, waited);
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         if (__syncthreads_or(!waited)) {
-            if (tid == 0) (void)mbar_wait(&s_bar, phase);
+            if (tid == 0) (void)mbar_wait(&s_bar[pb], (uint32_t)(((it - 1) >> 1) & 1));
             __syncthreads();
             ok = false;
-            break;
         }
-        phase ^= 1u;
     }
     if (!ok && tid == 0) atomicExch(&g_cnn_err, 1);
     __syncwarp();
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCOLS));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TCOLS));
     }
 }
 
@@ -537,20 +581,21 @@ unsigned grid_n(long long n, int bs)
 template <int CI, int CO>
 cudaError_t conv_launch(const ConvArgs &a, cudaStream_t s)
 {
-    const size_t sm = 16 * ((size_t)9 * (CI / 8) * CO + (size_t)3 * (CI / 8) * kShift);
+    // weights and two buffers of the three shifted halo copies
+    const size_t sm = 16 * ((size_t)9 * (CI / 8) * CO + (size_t)2 * 3 * (CI / 8) * kShift);
     auto k = conv3x3_kernel<CI, CO>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kCT, sm);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kCTC, sm);
     if (e != cudaSuccess) return e;
-    // resident CTAs each hold max(CO, 32) of the SM's 512 TMEM columns
-    per_sm = std::max(1, std::min(per_sm, 512 / std::max(CO, 32)));
+    // resident CTAs each hold two accumulators of max(CO, 32) of the SM's 512 TMEM columns
+    per_sm = std::max(1, std::min(per_sm, 512 / (2 * std::max(CO, 32))));
     const long long ntiles = (long long)a.B * ((a.H + kTH - 1) / kTH) * ((a.W + kTW - 1) / kTW);
     const unsigned grid = (unsigned)std::min<long long>(ntiles, (long long)sms * per_sm);
-    k<<<grid, kCT, sm, s>>>(a);
+    k<<<grid, kCTC, sm, s>>>(a);
     return cudaGetLastError();
 }
 
