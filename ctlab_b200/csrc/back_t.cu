@@ -64,6 +64,16 @@ constexpr size_t kSmemPerCta = 200 * 1024; // one CTA per SM
 constexpr size_t kStaticSmem = 20 * 1024;
 constexpr int kGeo = 4;               // geometry slots (views l .. l+3)
 
+// Column slot of column (cx, cy) in a row of the piece table: a permutation
+// of the 64 columns whose value mod 16 (the bank pair of an 8-byte entry)
+// differs within every 8 x 2 block {cx} x {2h, 2h+1} -- the 16 columns of a
+// half-warp of phase B -- and within every 4 x 4 quadrant -- the 16 columns
+// of a half-warp of phase A.
+__host__ __device__ constexpr int e_slot(int cx, int cy)
+{
+    return 16 * (cy >> 1) + ((cx ^ (4 * ((cy >> 1) & 1))) + 8 * (cy & 1));
+}
+
 __device__ __forceinline__ float lds_f32(uint32_t addr)
 {
     float v;
@@ -396,16 +406,18 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
     for (int r = 0; r < KSEG; ++r) acc[r] = 0.f;
     bool timed_out = false;
     const uint32_t E2_addr = smem_addr(E2);
-    // phase A: kAPh threads per column, each a run of vpt consecutive rows;
-    // a warp's lanes are 32 columns with the same run, so its table stores
-    // (consecutive columns of one row) hit distinct banks (with 8 columns x
-    // 4 runs a warp, they conflicted: 45.4 vs 42.1 ms at 512x512x256 / 984
-    // views)
+    // phase A: kAPh threads per column, each a run of vpt consecutive rows.
+    // A warp's lanes are 32 columns with the same run, 4 across the view's
+    // detector axis x 8 along it, so the P rows its strips read lie within a
+    // few cells (distinct banks: the row pitch is 4 mod 8 floats), and its
+    // table stores (column slots e_slot) hit distinct banks.  (With 8
+    // columns x 4 runs a warp the stores conflicted: 45.4 vs 42.1 ms at
+    // 512x512x256 / 984 views.)
     constexpr int kAPh = ZS;
-    const int ac = tid % kCols, aph = tid / kCols;
-    const int acx = ac & (kB - 1), acy = ac / kB;
+    const int aph = tid / kCols, alane = tid & 31, ahalf = (tid >> 5) & 1;
     const int i0 = aph * VPT; // this thread's entries i0 .. i0+VPT-1 (kAPh*VPT > DNV)
     const float nfi0 = -(float)i0;
+    const int eslot_b = e_slot(cx, cy); // phase B's column
 
     for (int li = 0; li < n; ++li) {
         const int b = li & 1, ls = li % kGeo;
@@ -415,6 +427,11 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
         const int xdrv = s_xdrv[ls];
         const int eb = EB == 2 ? b : 0;
         float2 *E = E2 + (size_t)eb * kCols * es2; // double buffered: B(li) overlaps A(li+1)
+        // this thread's phase-A column: the detector u axis runs along x
+        // for y-driven views and along y for x-driven ones
+        const int across = (alane & 3) + 4 * ahalf, along = alane >> 2;
+        const int acx = xdrv ? along : across, acy = xdrv ? across : along;
+        const int ac = acx + kB * acy, eslot_a = e_slot(acx, acy);
 
         // ---- A: (E_c(i), E_c(i+1) - E_c(i)) for i in [0, DNV], E_c(DNV+1) = E_c(DNV) ----
         // the thread's column strip for this view, recomputed from s_u (the
@@ -466,7 +483,7 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
             const float wmv[3] = {__uint_as_float(q1.w), __uint_as_float(q2.x), __uint_as_float(q2.y)};
             // the warp runs its widest column's whole-cell count, the others with weight 0
             const int nmax = (int)__reduce_max_sync(0xffffffffu, q2.z);
-            const uint32_t eout = E2_addr + 8u * (uint32_t)((eb * es2 + i0) * kCols + ac);
+            const uint32_t eout = E2_addr + 8u * (uint32_t)((eb * es2 + i0) * kCols + eslot_a);
             switch (nmax) {
             case 0: phase_a_run<VPT, 0>(pa, pb, pm, wmv, wa, wb, nfi0, DNVf, eout); break;
             case 1: phase_a_run<VPT, 1>(pa, pb, pm, wmv, wa, wb, nfi0, DNVf, eout); break;
@@ -478,7 +495,7 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
                 const uint32_t vp4 = 4u * (uint32_t)vp;
                 const uint32_t sbase = smem_addr(pbuf + (size_t)b * rmax * vp) + 4u * (uint32_t)i0;
                 auto row = [&](int u) { return sbase + (uint32_t)min(max(u - ulo, 0), rows - 1) * vp4; };
-                float2 *Ec = E + ac;
+                float2 *Ec = E + eslot_a;
                 float e = 0.f;
                 for (int j = 0; j <= VPT; ++j) {
                     const uint32_t o = 4u * (uint32_t)j;
@@ -493,7 +510,7 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
             // footprint wider than a stage: P from global memory
             const Strip st = strip();
             const float *Pg = a.pv + (long long)(lb + li) * DNU * vp;
-            float2 *Ec = E + ac;
+            float2 *Ec = E + eslot_a;
             auto eval = [&](int i) {
                 float e = fmaf(st.wb, __ldg(Pg + (size_t)st.ib * vp + i), st.wa * __ldg(Pg + (size_t)st.ia * vp + i));
                 for (int m = 0; m < st.nm; ++m) e = fmaf(st.wm, __ldg(Pg + (size_t)(st.first + m) * vp + i), e);
@@ -519,7 +536,7 @@ __global__ void __launch_bounds__(kCols * ZS, ZS == 4 ? 2 : 1) dd3_back_t_kernel
         if (in_vol && !timed_out && (!ZSKIP || rows >= 0)) {
             const float V0 = s_V0[ls][col], V1 = s_V1[ls][col];
             // address of piece i of this column = bits(i + 2^23) * 8 kCols + base (mod 2^32)
-            const uint32_t base = E2_addr + 8u * (uint32_t)(eb * kCols * es2 + col) - 8u * kCols * 0x4B000000u;
+            const uint32_t base = E2_addr + 8u * (uint32_t)(eb * kCols * es2 + eslot_b) - 8u * kCols * 0x4B000000u;
             const float vb0 = fmaf(V1, (float)k0, V0);
             float prev = 0.f;
 #pragma unroll
