@@ -109,6 +109,16 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint3
            ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
+// The same for a K-major operand stored by TMA with a swizzle: rows of
+// `row` bytes (one swizzle atom wide), groups of 8 rows SBO = 8 row bytes
+// apart, layout type 2 (128-byte swizzle) or 6 (32-byte swizzle) in bits
+// [61, 64), LBO unused (1); the atoms 1024-byte aligned (base offset 0).
+__device__ __forceinline__ uint64_t umma_desc_sw(uint32_t addr, uint32_t sbo, uint32_t layout)
+{
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | (1ull << 16) | ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46) |
+           ((uint64_t)layout << 61);
+}
+
 // Instruction descriptor, kind::f16: FP32 accumulator (bits 4-5 = 1), A and
 // B BF16 (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at 24.
 template <int N>
@@ -152,20 +162,23 @@ __device__ int g_cnn_err; // a convolution's MMA wait ran out (read by ctlab_cnn
 // and run tile t-1's epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31
 // (one output pixel each) and half w / 4 of the output channels.
 template <int CI, int CO>
-__global__ void __launch_bounds__(kCTC, 1) conv3x3_kernel(ConvArgs a)
+__global__ void __launch_bounds__(kCTC, 1) conv3x3_kernel(ConvArgs a, const __grid_constant__ CUtensorMap tm_in)
 {
+    static_assert(CI == 16 || CI == 64, "pixel rows of 32 or 128 bytes (one swizzle atom)");
     constexpr int NCH = CI / 8;                 // 16-byte chunks per input pixel
     constexpr int TCOLS = CO < 32 ? 32 : CO;    // TMEM columns of one accumulator (a power of 2 >= 32)
-    constexpr uint32_t kPlane = kShift * 16;    // bytes of one chunk plane of a shifted tile
-    constexpr uint32_t kHaloBytes = 3 * NCH * kPlane; // the three shifted copies of one tile
+    constexpr uint32_t kRowB = CI * 2;           // bytes of one pixel: a swizzle atom's row
+    constexpr uint32_t kCopyBytes = kHH * kTW * kRowB; // one column-shifted copy, [10 rows x 16][CI]
+    constexpr uint32_t kHaloBytes = 3 * kCopyBytes;    // the three shifted copies of one tile
+    constexpr uint32_t kSwLayout = CI == 64 ? 2u : 6u; // 128- or 32-byte swizzle
     constexpr uint32_t kIdesc = umma_idesc_bf16_m128<CO>();
-    constexpr int kHalo = kHH * kHW * NCH, kPer = (kHalo + kCTC - 1) / kCTC; // halo chunks, per thread
     constexpr int kEH = CO >= 32 ? 2 : 1;       // epilogue channel halves (warps 4-7 take the second)
     constexpr int kECH = CO / kEH;              // channels per epilogue thread
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char *s_w = smem;                          // [9][NCH][CO] chunks
     unsigned char *s_a = smem + 9 * NCH * CO * 16;      // [2][3][NCH][kShift] chunks
-    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ __align__(8) uint64_t s_bar[2];  // MMAs of the tile in accumulator / halo buffer 0, 1 done
+    __shared__ __align__(8) uint64_t s_hbar[2]; // halo buffer 0, 1 landed
     __shared__ uint32_t s_tmem;
     __shared__ float s_bias[CO];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -199,6 +212,8 @@ __global__ void __launch_bounds__(kCTC, 1) conv3x3_kernel(ConvArgs a)
     if (tid == 0) {
         mbar_init(&s_bar[0], 1);
         mbar_init(&s_bar[1], 1);
+        mbar_init(&s_hbar[0], 1);
+        mbar_init(&s_hbar[1], 1);
         mbar_fence_init();
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); // weights visible to the tensor cores
@@ -210,43 +225,18 @@ __global__ void __launch_bounds__(kCTC, 1) conv3x3_kernel(ConvArgs a)
 
     const int tiles_y = (a.H + kTH - 1) / kTH, tiles_x = (a.W + kTW - 1) / kTW;
     const int ntiles = a.B * tiles_y * tiles_x;
-    // halo chunk i of tile `tile` into registers (zero outside the image)
-    uint4 hv[kPer];
-    auto load_halo = [&](int tile) {
+    // the halo of `tile` into buffer hb (thread 0): three TMA tile loads of
+    // the NHWC input, one per column shift dx, each box 10 rows x 16 columns
+    // x CI channels (pixel rows of one swizzle atom), zero outside the image
+    auto request_halo = [&](int tile, int hb) {
+        if (tid != 0 || tile >= ntiles) return;
         const int b = tile / (tiles_y * tiles_x), tr = tile % (tiles_y * tiles_x);
         const int y0 = (tr / tiles_x) * kTH, x0 = (tr % tiles_x) * kTW;
+        mbar_arrive_expect_tx(&s_hbar[hb], kHaloBytes);
 #pragma unroll
-        for (int u = 0; u < kPer; ++u) {
-            const int i = u * kCTC + tid;
-            const int q = i % (kHH * kHW), kc = i / (kHH * kHW);
-            const int row = q / kHW, col = q - row * kHW;
-            const int y = y0 - 1 + row, x = x0 - 1 + col;
-            hv[u] = make_uint4(0u, 0u, 0u, 0u);
-            if (tile < ntiles && i < kHalo && y >= 0 && y < a.H && x >= 0 && x < a.W)
-                hv[u] = *reinterpret_cast<const uint4 *>(a.in + (((size_t)b * a.H + y) * a.W + x) * CI + kc * 8);
-        }
-    };
-    // registers -> the three column-shifted tiles of buffer hb (halo column
-    // col -> column col - dx of copy dx)
-    auto store_halo = [&](int hb) {
-        unsigned char *dst = s_a + (size_t)hb * kHaloBytes;
-#pragma unroll
-        for (int u = 0; u < kPer; ++u) {
-            const int i = u * kCTC + tid;
-            const int q = i % (kHH * kHW), kc = i / (kHH * kHW);
-            const int row = q / kHW, col = q - row * kHW;
-            if (i < kHalo) {
-#pragma unroll
-                for (int dx = 0; dx < 3; ++dx) {
-                    const int c = col - dx;
-                    if (c >= 0 && c < kTW)
-                        *reinterpret_cast<uint4 *>(dst + (size_t)(dx * NCH + kc) * kPlane + (size_t)(row * kTW + c) * 16) =
-                            hv[u];
-                }
-            }
-        }
-        // generic-proxy stores visible to the tensor cores (async proxy)
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        for (int dx = 0; dx < 3; ++dx)
+            tma_load_4d(s_a + (size_t)hb * kHaloBytes + (size_t)dx * kCopyBytes, &tm_in, 0, x0 - 1 + dx, y0 - 1, b,
+                        &s_hbar[hb]);
     };
     // tile's MMAs (thread 0): A from halo buffer hb, accumulator hb, committed to s_bar[hb]
     auto issue_mma = [&](int hb) {
@@ -258,8 +248,9 @@ __global__ void __launch_bounds__(kCTC, 1) conv3x3_kernel(ConvArgs a)
             const int dy = t / 3, dx = t - dy * 3;
 #pragma unroll
             for (int kk = 0; kk < CI / 16; ++kk) {
-                const uint64_t ad = umma_desc(a_hb + (uint32_t)(dx * NCH + 2 * kk) * kPlane + (uint32_t)(dy * kTW) * 16,
-                                              kPlane, 128);
+                const uint64_t ad = umma_desc_sw(a_hb + (uint32_t)dx * kCopyBytes + (uint32_t)(dy * kTW) * kRowB +
+                                                     (uint32_t)kk * 32u,
+                                                 8 * kRowB, kSwLayout);
                 const uint64_t bd = umma_desc(w_addr + (uint32_t)((t * NCH + 2 * kk) * CO) * 16, CO * 16, 128);
                 umma_bf16(tmem + (uint32_t)(hb * TCOLS), ad, bd, kIdesc, (t | kk) != 0);
             }
@@ -321,41 +312,52 @@ __global__ void __launch_bounds__(kCTC, 1) conv3x3_kernel(ConvArgs a)
         }
     };
 
-    // Iteration it (tile `tile`): halo into buffer it & 1 (its previous
-    // reader, the MMAs of iteration it - 2, completed: every thread waited
-    // for them in iteration it - 1), issue the tile's MMAs, load the next
-    // tile's halo, then wait for the previous tile's MMAs and run its
-    // epilogue while this tile's MMAs run.  Accumulator it & 1 was last read
-    // by the epilogue of iteration it - 2, finished before this iteration's
-    // barrier.  Any wait that runs out stops the whole CTA (no further halo
-    // stores or MMAs) after bounded waits for the MMAs in flight, so that
-    // tensor memory is not freed under them; the launch's output is invalid
-    // once g_cnn_err is set.
-    bool ok = true;
+    // Iteration it (tile `tile`, buffers it & 1): thread 0 waits for the
+    // tile's halo and issues its MMAs; every thread waits for the previous
+    // tile's MMAs, after which thread 0 requests the next tile's halo into
+    // the buffer they read, and the warps run the previous tile's epilogue
+    // while this tile's MMAs run.  Accumulator it & 1 was last read by the
+    // epilogue of iteration it - 2, finished before the last barrier.  Any
+    // wait that runs out stops the whole CTA (no further copies or MMAs)
+    // after bounded waits for the copies and MMAs in flight, so that neither
+    // lands in freed memory; the launch's output is invalid once g_cnn_err
+    // is set.  The swizzled halo copies need 1024-byte aligned buffers: a
+    // misaligned one stops the CTA before any copy.
+    bool ok = (a_addr & 1023u) == 0;
     int it = 0, prev_tile = -1;
-    load_halo(blockIdx.x);
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+    if (ok) request_halo(blockIdx.x, 0);
+    for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x, ++it) {
         const int hb = it & 1;
-        store_halo(hb);
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
-        issue_mma(hb);
-        load_halo(tile + gridDim.x);
+        bool mine = true; // thread 0: the halo landed and the MMAs went out
+        if (tid == 0) {
+            mine = mbar_wait(&s_hbar[hb], (uint32_t)((it >> 1) & 1));
+            if (mine) issue_mma(hb);
+        }
+        bool waited = true, requested = false;
         if (it >= 1) {
-            const bool waited = mbar_wait(&s_bar[hb ^ 1], (uint32_t)(((it - 1) >> 1) & 1));
+            waited = mbar_wait(&s_bar[hb ^ 1], (uint32_t)(((it - 1) >> 1) & 1));
+            if (tid == 0 && waited && mine) {
+                request_halo(tile + gridDim.x, hb ^ 1);
+                requested = tile + gridDim.x < ntiles;
+            }
             __syncwarp();
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             epilogue(prev_tile, hb ^ 1, waited);
-            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            if (__syncthreads_or(!waited)) {
-                if (tid == 0) {
-                    (void)mbar_wait(&s_bar[hb], (uint32_t)((it >> 1) & 1));
-                    (void)mbar_wait(&s_bar[hb ^ 1], (uint32_t)(((it - 1) >> 1) & 1));
-                }
-                __syncthreads();
-                ok = false;
-                break;
+        } else if (tid == 0 && mine) {
+            request_halo(tile + gridDim.x, 1); // buffer 1 not read yet
+            requested = tile + gridDim.x < ntiles;
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        if (__syncthreads_or(!waited || !mine)) {
+            if (tid == 0) {
+                if (mine) (void)mbar_wait(&s_bar[hb], (uint32_t)((it >> 1) & 1));
+                else (void)mbar_wait(&s_hbar[hb], (uint32_t)((it >> 1) & 1));
+                if (it >= 1) (void)mbar_wait(&s_bar[hb ^ 1], (uint32_t)(((it - 1) >> 1) & 1));
+                if (requested) (void)mbar_wait(&s_hbar[hb ^ 1], (uint32_t)(((it + 1) >> 1) & 1));
             }
+            __syncthreads();
+            ok = false;
+            break;
         }
         prev_tile = tile;
     }
@@ -595,7 +597,17 @@ cudaError_t conv_launch(const ConvArgs &a, cudaStream_t s)
     per_sm = std::max(1, std::min(per_sm, 512 / (2 * std::max(CO, 32))));
     const long long ntiles = (long long)a.B * ((a.H + kTH - 1) / kTH) * ((a.W + kTW - 1) / kTW);
     const unsigned grid = (unsigned)std::min<long long>(ntiles, (long long)sms * per_sm);
-    k<<<grid, kCTC, sm, s>>>(a);
+    // the NHWC input, boxes of 10 rows x 16 columns x CI channels, each pixel
+    // a swizzle atom's row (128-byte swizzle for 64 channels, 32-byte for 16)
+    CUtensorMap tm;
+    const cuuint64_t dims[4] = {(cuuint64_t)CI, (cuuint64_t)a.W, (cuuint64_t)a.H, (cuuint64_t)a.B};
+    const cuuint64_t strides[3] = {(cuuint64_t)CI * 2, (cuuint64_t)a.W * CI * 2, (cuuint64_t)a.H * a.W * CI * 2};
+    const cuuint32_t box[4] = {(cuuint32_t)CI, (cuuint32_t)kTW, (cuuint32_t)kHH, 1};
+    if (encode_tiled_map(&tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16 *>(a.in), dims, strides, box,
+                         CI == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_32B,
+                         "a convolution input") != CTLAB_OK)
+        return cudaErrorInvalidValue;
+    k<<<grid, kCTC, sm, s>>>(a, tm);
     return cudaGetLastError();
 }
 

@@ -140,6 +140,13 @@ cudaError_t launch_zt_rows(const float *vol, const unsigned char *mask, int XN, 
 // The prefixes Z[k] = P + k f of a pair array [planes][rows][rs] into out.
 cudaError_t launch_zt_unpack(const float2 *in, float *out, int planes, int rows, int rs, cudaStream_t s);
 
+// A tiled TMA map (no interleave, zero fill outside the tensor): rank <= 5,
+// dims[0] contiguous, strides in bytes of dims 1 .. rank-1 (multiples of
+// 16), box extents per dim, the given shared-memory swizzle.  Returns a
+// status.
+int encode_tiled_map(CUtensorMap *m, CUtensorMapDataType dtype, int rank, void *base, const cuuint64_t *dims,
+                     const cuuint64_t *strides, const cuuint32_t *box, CUtensorMapSwizzle swizzle, const char *what);
+
 // Projection SAT: Q[p][u'][v'] of W = prj * L (L = slab path weight of the
 // view's driving axis) for n views of the list.
 // Projection rows weighted by the slab path length L of the view's driving

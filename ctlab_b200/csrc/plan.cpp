@@ -67,6 +67,18 @@ int encode_zt_map(CUtensorMap *m, float2 *base, int nb, int ZN, int na, int rs, 
 
 } // namespace
 
+int encode_tiled_map(CUtensorMap *m, CUtensorMapDataType dtype, int rank, void *base, const cuuint64_t *dims,
+                     const cuuint64_t *strides, const cuuint32_t *box, CUtensorMapSwizzle swizzle, const char *what)
+{
+    PFN_cuTensorMapEncodeTiled_v12000 fn = tensor_map_encoder();
+    if (!fn) return set_status(CTLAB_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+    const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+    const CUresult r = fn(m, dtype, (cuuint32_t)rank, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_status(CTLAB_ERR_CUDA, std::string("cuTensorMapEncodeTiled failed for ") + what);
+    return CTLAB_OK;
+}
+
 void plan_free(ctlab_plan *p)
 {
     if (!p) return;
