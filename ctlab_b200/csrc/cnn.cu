@@ -93,10 +93,12 @@ struct ConvArgs {
 
 // ---- 5th-generation tensor cores (tcgen05): one M = 128 x N = CO x K = 16 MMA
 // per (tap, 16 input channels), operands in shared memory, FP32 accumulator
-// in tensor memory.  Shared-memory operand layout (K-major, no swizzle):
-// 16-byte chunks of 8 channels, the rows of a chunk plane 16 bytes apart,
-// groups of 8 rows SBO bytes apart, the two 8-channel halves of an MMA's K
-// LBO bytes apart.
+// in tensor memory.  Both operands are K-major.  B (the weights, stored by
+// the threads) has no swizzle: 16-byte chunks of 8 channels, the rows of a
+// chunk plane 16 bytes apart, groups of 8 rows SBO bytes apart, the two
+// 8-channel halves of an MMA's K LBO bytes apart.  A (the input halo, stored
+// by TMA) is one pixel per row of CI * 2 bytes in the 128-byte (CI = 64) or
+// 32-byte (CI = 16) swizzle, addressed by umma_desc_sw.
 
 constexpr int kTPix = kTH * kTW;       // 128 output pixels: the MMA's M
 constexpr int kShift = kHH * kTW;      // 160 pixels of one column-shifted input tile (10 rows x 16)
@@ -154,13 +156,15 @@ __device__ int g_cnn_err; // a convolution's MMA wait ran out (read by ctlab_cnn
 // 3x3 convolution, implicit GEMM on tcgen05: per tile of 8 x 16 output
 // pixels, M = 128 pixels, N = CO, K = 9 taps x CI.  The CTA keeps the layer's
 // weights in shared memory as [tap][chunk][co] and, per tile, three copies of
-// the input halo shifted by one column each, [dx][chunk][10 rows x 16]: the
-// A operand of tap (dy, dx) is then the 128 consecutive rows of copy dx from
-// row dy, a plain descriptor.  Thread 0 issues the 9 * CI/16 MMAs and
-// commits them to an mbarrier.  Halo copies and TMEM accumulators are double
-// buffered, so the MMAs of tile t run while the 8 warps load tile t+1's halo
-// and run tile t-1's epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31
-// (one output pixel each) and half w / 4 of the output channels.
+// the input halo shifted by one column each, [dx][10 rows x 16 pixels][CI]
+// in swizzled pixel rows, each loaded by one TMA tile load (zero fill outside
+// the image): the A operand of tap (dy, dx) is then the 128 consecutive
+// pixel rows of copy dx from row dy, one swizzled descriptor.  Thread 0
+// issues the 9 * CI/16 MMAs and commits them to an mbarrier.  Halo copies and
+// TMEM accumulators are double buffered, so the MMAs of tile t run while
+// thread 0 requests tile t+1's halo and the 8 warps run tile t-1's epilogue:
+// warp w reads TMEM lanes 32 (w % 4) .. + 31 (one output pixel each) and
+// half w / 4 of the output channels.
 template <int CI, int CO>
 __global__ void __launch_bounds__(kCTC, 1) conv3x3_kernel(ConvArgs a, const __grid_constant__ CUtensorMap tm_in)
 {
@@ -176,7 +180,7 @@ __global__ void __launch_bounds__(kCTC, 1) conv3x3_kernel(ConvArgs a, const __gr
     constexpr int kECH = CO / kEH;              // channels per epilogue thread
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char *s_w = smem;                          // [9][NCH][CO] chunks
-    unsigned char *s_a = smem + 9 * NCH * CO * 16;      // [2][3][NCH][kShift] chunks
+    unsigned char *s_a = smem + 9 * NCH * CO * 16;      // [2][3][kShift pixels][CI], swizzled
     __shared__ __align__(8) uint64_t s_bar[2];  // MMAs of the tile in accumulator / halo buffer 0, 1 done
     __shared__ __align__(8) uint64_t s_hbar[2]; // halo buffer 0, 1 landed
     __shared__ uint32_t s_tmem;
