@@ -41,9 +41,10 @@ namespace {
 typedef __nv_bfloat16 bf16;
 
 constexpr int kTH = 8, kTW = 16;               // output tile of a CTA: 8 rows x 16 columns
-constexpr int kHH = kTH + 2, kHW = kTW + 2;    // input halo tile
+constexpr int kHH = kTH + 2;                   // input halo rows
 constexpr int kCT = 128;                       // 4 warps, two tile rows each (weight gradient)
-constexpr int kCTC = 256;                      // convolution CTA: 8 warps
+constexpr int kCTC = 256;                      // convolution CTA: 8 epilogue warps ...
+constexpr int kCTP = kCTC + 32;                // ... and the producer warp
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
 {
@@ -59,12 +60,6 @@ __device__ __forceinline__ int swz(int r, int c)
     else return c ^ ((r >> 2) & (CH - 1));
 }
 
-__device__ __forceinline__ void ldsm_x4(uint32_t addr, uint32_t &r0, uint32_t &r1, uint32_t &r2, uint32_t &r3)
-{
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];"
-                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
-                 : "r"(addr));
-}
 __device__ __forceinline__ void ldsm_x4_t(uint32_t addr, uint32_t &r0, uint32_t &r1, uint32_t &r2, uint32_t &r3)
 {
     asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0, %1, %2, %3}, [%4];"
@@ -159,14 +154,15 @@ __device__ int g_cnn_err; // a convolution's MMA wait ran out (read by ctlab_cnn
 // the input halo shifted by one column each, [dx][10 rows x 16 pixels][CI]
 // in swizzled pixel rows, each loaded by one TMA tile load (zero fill outside
 // the image): the A operand of tap (dy, dx) is then the 128 consecutive
-// pixel rows of copy dx from row dy, one swizzled descriptor.  Thread 0
-// issues the 9 * CI/16 MMAs and commits them to an mbarrier.  Halo copies and
-// TMEM accumulators are double buffered, so the MMAs of tile t run while
-// thread 0 requests tile t+1's halo and the 8 warps run tile t-1's epilogue:
-// warp w reads TMEM lanes 32 (w % 4) .. + 31 (one output pixel each) and
-// half w / 4 of the output channels.
+// pixel rows of copy dx from row dy, one swizzled descriptor.  One producer
+// thread (lane 0 of warp 8) requests the halos and issues each tile's
+// 9 * CI/16 MMAs, committed to an mbarrier; warps 0 .. 7 run the epilogues
+// (warp w reads TMEM lanes 32 (w % 4) .. + 31, one output pixel each, and
+// half w / 4 of the output channels).  Halo copies and TMEM accumulators are
+// double buffered and the two roles meet only at mbarriers, so the MMAs of
+// tile t, the copy of tile t+1's halo and the epilogue of tile t-1 overlap.
 template <int CI, int CO>
-__global__ void __launch_bounds__(kCTC, 1) conv3x3_kernel(ConvArgs a, const __grid_constant__ CUtensorMap tm_in)
+__global__ void __launch_bounds__(kCTP, 1) conv3x3_kernel(ConvArgs a, const __grid_constant__ CUtensorMap tm_in)
 {
     static_assert(CI == 16 || CI == 64, "pixel rows of 32 or 128 bytes (one swizzle atom)");
     constexpr int NCH = CI / 8;                 // 16-byte chunks per input pixel
@@ -183,14 +179,17 @@ __global__ void __launch_bounds__(kCTC, 1) conv3x3_kernel(ConvArgs a, const __gr
     unsigned char *s_a = smem + 9 * NCH * CO * 16;      // [2][3][kShift pixels][CI], swizzled
     __shared__ __align__(8) uint64_t s_bar[2];  // MMAs of the tile in accumulator / halo buffer 0, 1 done
     __shared__ __align__(8) uint64_t s_hbar[2]; // halo buffer 0, 1 landed
+    __shared__ __align__(8) uint64_t s_tfree[2]; // accumulator 0, 1 read out (one arrival per epilogue warp)
     __shared__ uint32_t s_tmem;
+    __shared__ int s_abort; // a wait ran out: both roles stop
     __shared__ float s_bias[CO];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid < CO) s_bias[tid] = a.bias ? a.bias[tid] : 0.f;
+    if (tid == 0) s_abort = 0;
 
     // the layer's weights, 12 loads in flight per thread
     constexpr int kWChunks = CO * 9 * NCH;
-    for (int i0 = 0; i0 < kWChunks; i0 += 12 * kCTC) {
+    for (int i0 = 0; tid < kCTC && i0 < kWChunks; i0 += 12 * kCTC) {
         uint4 v[12];
 #pragma unroll
         for (int u = 0; u < 12; ++u) {
@@ -218,6 +217,8 @@ __global__ void __launch_bounds__(kCTC, 1) conv3x3_kernel(ConvArgs a, const __gr
         mbar_init(&s_bar[1], 1);
         mbar_init(&s_hbar[0], 1);
         mbar_init(&s_hbar[1], 1);
+        mbar_init(&s_tfree[0], kCTC / 32);
+        mbar_init(&s_tfree[1], kCTC / 32);
         mbar_fence_init();
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); // weights visible to the tensor cores
@@ -229,11 +230,10 @@ __global__ void __launch_bounds__(kCTC, 1) conv3x3_kernel(ConvArgs a, const __gr
 
     const int tiles_y = (a.H + kTH - 1) / kTH, tiles_x = (a.W + kTW - 1) / kTW;
     const int ntiles = a.B * tiles_y * tiles_x;
-    // the halo of `tile` into buffer hb (thread 0): three TMA tile loads of
+    // the halo of `tile` into buffer hb (producer): three TMA tile loads of
     // the NHWC input, one per column shift dx, each box 10 rows x 16 columns
     // x CI channels (pixel rows of one swizzle atom), zero outside the image
     auto request_halo = [&](int tile, int hb) {
-        if (tid != 0 || tile >= ntiles) return;
         const int b = tile / (tiles_y * tiles_x), tr = tile % (tiles_y * tiles_x);
         const int y0 = (tr / tiles_x) * kTH, x0 = (tr % tiles_x) * kTW;
         mbar_arrive_expect_tx(&s_hbar[hb], kHaloBytes);
@@ -242,12 +242,11 @@ __global__ void __launch_bounds__(kCTC, 1) conv3x3_kernel(ConvArgs a, const __gr
             tma_load_4d(s_a + (size_t)hb * kHaloBytes + (size_t)dx * kCopyBytes, &tm_in, 0, x0 - 1 + dx, y0 - 1, b,
                         &s_hbar[hb]);
     };
-    // tile's MMAs (thread 0): A from halo buffer hb, accumulator hb, committed to s_bar[hb]
+    // tile's MMAs (producer): A from halo buffer hb, accumulator hb, committed to s_bar[hb]
     auto issue_mma = [&](int hb) {
-        if (tid != 0) return;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t a_hb = a_addr + (uint32_t)hb * kHaloBytes;
-#pragma unroll 1
+#pragma unroll
         for (int t = 0; t < 9; ++t) {
             const int dy = t / 3, dx = t - dy * 3;
 #pragma unroll
@@ -265,7 +264,7 @@ __global__ void __launch_bounds__(kCTC, 1) conv3x3_kernel(ConvArgs a, const __gr
     };
     // epilogue of `tile` from accumulator ab: accumulator row m = 32 (warp % 4)
     // + lane is output pixel (m / 16, m % 16); this warp's channel half
-    auto epilogue = [&](int tile, int ab, bool valid) {
+    auto epilogue = [&](int tile, int ab) {
         const int half = warp >> 2;
         if (half >= kEH) return; // warp-uniform
         const int b = tile / (tiles_y * tiles_x), tr = tile % (tiles_y * tiles_x);
@@ -281,7 +280,7 @@ __global__ void __launch_bounds__(kCTC, 1) conv3x3_kernel(ConvArgs a, const __gr
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         const int m = (warp & 3) * 32 + lane;
         const int y = y0 + m / kTW, x = x0 + m % kTW;
-        if (!valid || y >= a.H || x >= a.W) return;
+        if (y >= a.H || x >= a.W) return;
         const size_t pix = ((size_t)b * a.H + y) * a.W + x;
         if (a.epi == CTLAB_CNN_EPI_RESIDUAL) {
             if (half == 0) a.out_f32[pix] = __uint_as_float(v[0]) + s_bias[0] + a.center[pix];
@@ -316,69 +315,77 @@ __global__ void __launch_bounds__(kCTC, 1) conv3x3_kernel(ConvArgs a, const __gr
         }
     };
 
-    // Iteration it (tile `tile`, buffers it & 1): thread 0 waits for the
-    // tile's halo and issues its MMAs; every thread waits for the previous
-    // tile's MMAs, after which thread 0 requests the next tile's halo into
-    // the buffer they read, and the warps run the previous tile's epilogue
-    // while this tile's MMAs run.  Accumulator it & 1 was last read by the
-    // epilogue of iteration it - 2, finished before the last barrier.  Any
-    // wait that runs out stops the whole CTA (no further copies or MMAs)
-    // after bounded waits for the copies and MMAs in flight, so that neither
-    // lands in freed memory; the launch's output is invalid once g_cnn_err
-    // is set.  The swizzled halo copies need 1024-byte aligned buffers: a
-    // misaligned one stops the CTA before any copy.
+    // Iteration it (tile `tile`) uses halo buffer and accumulator it & 1.
+    // The producer polls two conditions: the MMAs of it - 1 completed (the
+    // last reader of the other buffer), upon which it requests the halo of
+    // it + 1 there; and the halo of it landed with the accumulator released
+    // by the epilogue of it - 2, upon which it issues the MMAs of it.  The
+    // epilogue warps wait for the MMAs of each tile and release its
+    // accumulator.  A wait that runs out sets s_abort, which stops both
+    // roles; the producer then waits (bounded) for its MMAs and halo copies
+    // in flight, so that neither lands after the CTA frees its tensor and
+    // shared memory.  The launch's output is invalid once g_cnn_err is set.
+    // The swizzled halo copies need 1024-byte aligned buffers: a misaligned
+    // one stops the CTA before any copy.
+    const volatile int *abort_flag = &s_abort;
     bool ok = (a_addr & 1023u) == 0;
-    int it = 0, prev_tile = -1;
-    if (ok) request_halo(blockIdx.x, 0);
-    for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x, ++it) {
-        const int hb = it & 1;
-        bool mine = true; // thread 0: the halo landed and the MMAs went out
-        if (tid == 0) {
-            mine = mbar_wait(&s_hbar[hb], (uint32_t)((it >> 1) & 1));
-            if (mine) issue_mma(hb);
-        }
-        bool waited = true, requested = false;
-        if (it >= 1) {
-            waited = mbar_wait(&s_bar[hb ^ 1], (uint32_t)(((it - 1) >> 1) & 1));
-            if (tid == 0 && waited && mine) {
-                request_halo(tile + gridDim.x, hb ^ 1);
-                requested = tile + gridDim.x < ntiles;
+    if (warp == kCTC / 32) {
+        if (lane == 0 && ok) {
+            int it = 0, issued = 0, landed = 0, requested = 1; // MMA batches, halos seen landed, halos requested
+            request_halo(blockIdx.x, 0);
+            for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+                const int hb = it & 1;
+                bool need_req = tile + (int)gridDim.x < ntiles, need_mma = true;
+                for (uint32_t n = 0; (need_req || need_mma) && n < kMbarTestLimit; ++n) {
+                    if (need_req && (it == 0 || mbar_test_wait(&s_bar[hb ^ 1], (uint32_t)(((it - 1) >> 1) & 1)))) {
+                        request_halo(tile + gridDim.x, hb ^ 1);
+                        requested = it + 2;
+                        need_req = false;
+                    }
+                    if (need_mma && mbar_test_wait(&s_hbar[hb], (uint32_t)((it >> 1) & 1)) &&
+                        (it < 2 || mbar_test_wait(&s_tfree[hb], (uint32_t)(((it - 2) >> 1) & 1)))) {
+                        landed = it + 1;
+                        issue_mma(hb);
+                        issued = it + 1;
+                        need_mma = false;
+                    }
+                    if ((n & 1023u) == 1023u && *abort_flag) break;
+                }
+                if (need_req || need_mma) {
+                    ok = false;
+                    break;
+                }
             }
-            __syncwarp();
+            // drain: the last MMA commit covers every MMA issued; halos
+            // landed .. requested - 1 may still be in flight
+            if (issued > 0 && !mbar_wait(&s_bar[(issued - 1) & 1], (uint32_t)(((issued - 1) >> 1) & 1))) ok = false;
+            for (int k = landed; k < requested; ++k)
+                if (!mbar_wait(&s_hbar[k & 1], (uint32_t)((k >> 1) & 1))) ok = false;
+        }
+    } else {
+        int it = 0;
+        for (int tile = blockIdx.x; ok && tile < ntiles; tile += gridDim.x, ++it) {
+            const int hb = it & 1;
+            bool waited = false;
+            for (uint32_t n = 0; !waited && n < kMbarSpinLimit; ++n) {
+                waited = mbar_try_wait(&s_bar[hb], (uint32_t)((it >> 1) & 1));
+                if (!waited && (n & 255u) == 255u && *abort_flag) break;
+            }
+            if (!__all_sync(0xffffffffu, waited)) {
+                ok = false;
+                break;
+            }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            epilogue(prev_tile, hb ^ 1, waited);
-        } else if (tid == 0 && mine) {
-            request_halo(tile + gridDim.x, 1); // buffer 1 not read yet
-            requested = tile + gridDim.x < ntiles;
-        }
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        if (__syncthreads_or(!waited || !mine)) {
-            if (tid == 0) {
-                if (mine) (void)mbar_wait(&s_bar[hb], (uint32_t)((it >> 1) & 1));
-                else (void)mbar_wait(&s_hbar[hb], (uint32_t)((it >> 1) & 1));
-                if (it >= 1) (void)mbar_wait(&s_bar[hb ^ 1], (uint32_t)(((it - 1) >> 1) & 1));
-                if (requested) (void)mbar_wait(&s_hbar[hb ^ 1], (uint32_t)(((it + 1) >> 1) & 1));
-            }
-            __syncthreads();
-            ok = false;
-            break;
-        }
-        prev_tile = tile;
-    }
-    if (ok && it >= 1) {
-        const int pb = (it - 1) & 1;
-        const bool waited = mbar_wait(&s_bar[pb], (uint32_t)(((it - 1) >> 1) & 1));
-        __syncwarp();
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        epilogue(prev_tile, pb, waited);
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        if (__syncthreads_or(!waited)) {
-            if (tid == 0) (void)mbar_wait(&s_bar[pb], (uint32_t)(((it - 1) >> 1) & 1));
-            __syncthreads();
-            ok = false;
+            epilogue(tile, hb);
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&s_tfree[hb]);
         }
     }
-    if (!ok && tid == 0) atomicExch(&g_cnn_err, 1);
+    if (!ok && lane == 0) s_abort = 1;
+    __syncwarp();
+    __syncthreads();
+    if (tid == 0 && s_abort) atomicExch(&g_cnn_err, 1);
     __syncwarp();
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -595,7 +602,7 @@ cudaError_t conv_launch(const ConvArgs &a, cudaStream_t s)
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kCTC, sm);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kCTP, sm);
     if (e != cudaSuccess) return e;
     // resident CTAs each hold two accumulators of max(CO, 32) of the SM's 512 TMEM columns
     per_sm = std::max(1, std::min(per_sm, 512 / (2 * std::max(CO, 32))));
@@ -611,7 +618,7 @@ cudaError_t conv_launch(const ConvArgs &a, cudaStream_t s)
                          CI == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_32B,
                          "a convolution input") != CTLAB_OK)
         return cudaErrorInvalidValue;
-    k<<<grid, kCTC, sm, s>>>(a, tm);
+    k<<<grid, kCTP, sm, s>>>(a, tm);
     return cudaGetLastError();
 }
 

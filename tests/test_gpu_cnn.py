@@ -35,7 +35,9 @@ def from_bf16_dev(t):
     return (t.view(torch.int16).cpu().numpy().astype(np.uint16).astype(np.uint32) << 16).view(np.float32)
 
 
-SHAPES = [(2, 12, 20), (1, 9, 33)]  # partial 8x16 tiles on purpose
+# partial 8x16 tiles on purpose; the last shape gives every persistent CTA
+# three or more tiles, so both halo buffers and accumulators are reused
+SHAPES = [(2, 12, 20), (1, 9, 33), (8, 72, 200)]
 
 
 @pytest.mark.parametrize("ci,co", [(16, 64), (64, 64), (64, 16)])
