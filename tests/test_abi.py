@@ -107,3 +107,19 @@ def test_random_ellipsoids_are_seeded_and_in_range():
     assert np.all((a[:, 4] >= 0.05 * 256) & (a[:, 4] <= 0.4 * 256))
     assert np.all((a[:, 0] >= 0) & (a[:, 0] <= 0.03))
     assert np.all((a[:, 7:] >= 0) & (a[:, 7:] <= np.pi))
+
+
+def test_cnn_entry_points_reject_bad_arguments_on_host():
+    # never dereferenced: every call below returns before any CUDA call
+    lib, p = cb.load(), C.c_void_p(16)
+    inv, uns = cb.CTLAB_ERR_INVALID_ARG, cb.CTLAB_ERR_UNSUPPORTED
+    relu, mask, resid = 0, 1, 2
+    assert lib.ctlab_cnn_conv(None, 64, p, p, 64, 1, 8, 8, relu, p, None, None, None, None) == inv
+    assert lib.ctlab_cnn_conv(p, 64, p, p, 64, 0, 8, 8, relu, p, None, None, None, None) == inv
+    assert lib.ctlab_cnn_conv(p, 64, p, None, 64, 1, 8, 8, relu, p, None, None, None, None) == inv  # no bias
+    assert lib.ctlab_cnn_conv(p, 64, p, p, 64, 1, 8, 8, mask, p, None, None, None, None) == inv  # no mask
+    assert lib.ctlab_cnn_conv(p, 64, p, p, 16, 1, 8, 8, resid, None, None, p, None, None) == inv  # no centre
+    assert lib.ctlab_cnn_conv(p, 32, p, p, 64, 1, 8, 8, relu, p, None, None, None, None) == uns
+    assert "channels" in lib.ctlab_last_error().decode()
+    assert lib.ctlab_cnn_wgrad(p, 64, None, 64, 1, 8, 8, p, None, None) == inv
+    assert lib.ctlab_cnn_wgrad(p, 64, p, 32, 1, 8, 8, p, None, None) == uns
