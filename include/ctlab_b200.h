@@ -48,11 +48,14 @@ extern "C" {
 
 /* Summed-area-table arithmetic of a plan.  FP64: 2-D FP64 prefix sums of the
  * volume slices and projections; F32PAIR: the same as compensated FP32 pairs
- * (hi+lo float-float sums); both 8 bytes per entry.  ZPREFIX: the projector
- * stages per-column z prefix sums (FP64 sums rounded to FP32, 4 bytes),
- * slice-major per driving axis, and forms the in-plane integral from
- * adjacent columns -- the same FP32 quantities the 2-D FP64 path forms after
- * its column differences; the backprojector keeps FP64 projection SATs. */
+ * (hi+lo float-float sums); both 8 bytes per entry.  ZPREFIX (the default of
+ * the legacy entry points and of the Python Plan): the projector stages
+ * per-column z prefix sums accumulated in FP64, slice-major per driving axis,
+ * as affine pieces (P, f) of two FP32 values (the prefix at kz is P + kz f),
+ * and forms the in-plane integral from adjacent columns -- the same FP32
+ * quantities the 2-D FP64 path forms after its column differences; the
+ * backprojector likewise reads per-detector-column v prefix sums of the
+ * weighted projections, accumulated in FP64 and stored in FP32. */
 #define CTLAB_SAT_FP64 0
 #define CTLAB_SAT_F32PAIR 1
 #define CTLAB_SAT_ZPREFIX 2
@@ -134,8 +137,8 @@ typedef struct ctlab_geometry {
 typedef struct ctlab_plan ctlab_plan;
 
 /* Validates the geometry, uploads per-view constants and allocates the SAT
- * workspaces on `device`.  sat_mode is CTLAB_SAT_FP64 or
- * CTLAB_SAT_F32PAIR.  The plan is used from one stream at a time.
+ * workspaces on `device`.  sat_mode is CTLAB_SAT_FP64, CTLAB_SAT_F32PAIR or
+ * CTLAB_SAT_ZPREFIX.  The plan is used from one stream at a time.
  * New in this library (the reference recomputes everything per call). */
 int ctlab_plan_create(const ctlab_geometry *geom, int device, int sat_mode, ctlab_plan **out);
 int ctlab_plan_destroy(ctlab_plan *plan);
