@@ -11,7 +11,16 @@ FP64 rounding: the integral of a piecewise-constant field is bilinear inside
 each cell, so the bilinear SAT sample is exact.  The view frames come from the
 oracle's own make_view (pinned to the reference's rotation in
 test_oracle_golden.py) and the detector boundaries from orc_dd3_boundaries
-(pinned to DD3Boundaries); what this file checks is the integration."""
+(pinned to DD3Boundaries); what this file checks is the integration.
+
+A second, looser check compares the oracle's branchless projection with the
+conventional 3-D distance-driven projection for a flat (equal-distance)
+detector -- the model DDM3D_ED_proj declares (src/DDM_proj.h:57-82), whose
+body the reference does not ship -- restated from the published method:
+in-plane overlaps as above, but each voxel column's z overlap taken at that
+column's own magnification (the ray from the source through the column's
+centre) rather than along the cell's central ray.  The two models differ
+only by the magnification's variation across one strip."""
 import ctypes as C
 
 import numpy as np
@@ -125,6 +134,53 @@ def back_direct(g, prj, mask=None):
     return out.reshape(g.YN, g.XN, g.ZN)
 
 
+def proj_conventional(g, vol, mask=None):
+    f = np.asarray(vol, np.float32).astype(np.float64).reshape(g.YN, g.XN, g.ZN)
+    if mask is not None:
+        f = f * (np.asarray(mask).reshape(g.YN, g.XN, 1) != 0)
+    bx, by, bz = _boundaries(g)
+    xds, yds, zds = (np.asarray(a, np.float32).astype(np.float64) for a in (g.xds, g.yds, g.zds))
+    x_lo = g.imgXCenter - 0.5 * g.XN * g.dx
+    y_lo = g.imgYCenter - 0.5 * g.YN * g.dx
+    z_lo = g.imgZCenter - 0.5 * g.ZN * g.dz
+    Ex_l, Ey_l = (bx[-1] - bx[0]) / g.DNU, (by[-1] - by[0]) / g.DNU
+    k = np.arange(g.ZN)
+    out = np.zeros((g.PN, g.DNU, g.DNV))
+    for p in range(g.PN):
+        c, s, zP, Sx, Sy, Sz, xdrv = _frame(g, p)
+        rot = lambda x, y: (x * c - y * s, x * s + y * c)
+        B0x, B0y = rot(bx[0], by[0])
+        Ex, Ey = rot(Ex_l, Ey_l)
+        if xdrv:
+            F, NA, NB, a_c, b_c, b_lo, Sa, Sb = f.transpose(1, 0, 2), g.XN, g.YN, g.imgXCenter, g.imgYCenter, y_lo, Sx, Sy
+        else:
+            F, NA, NB, a_c, b_c, b_lo, Sa, Sb = f, g.YN, g.XN, g.imgYCenter, g.imgXCenter, x_lo, Sy, Sx
+        aj = a_c + (np.arange(NA) - 0.5 * (NA - 1)) * g.dx
+        bi = b_c + (np.arange(NB) - 0.5 * (NB - 1)) * g.dx
+        A, Bm = np.meshgrid(aj, bi, indexing="ij")  # (NA, NB) voxel column centres
+        PX, PY = (A, Bm) if xdrv else (Bm, A)
+        # the ray from the source through each column centre meets the flat
+        # detector at S + lam (P - S): the column's magnification is lam
+        lam = ((B0x - Sx) * Ey - (B0y - Sy) * Ex) / ((PX - Sx) * Ey - (PY - Sy) * Ex)
+        da = aj - Sa
+        for u in range(g.DNU):
+            B0, B1, Cw = rot(bx[u], by[u]), rot(bx[u + 1], by[u + 1]), rot(xds[u], yds[u])
+            ab = (lambda P: (P[0], P[1])) if xdrv else (lambda P: (P[1], P[0]))
+            (B0a, B0b), (B1a, B1b) = ab(B0), ab(B1)
+            xa = (Sb + da / (B0a - Sa) * (B0b - Sb) - b_lo) / g.dx
+            xb = (Sb + da / (B1a - Sa) * (B1b - Sb) - b_lo) / g.dx
+            wx = _overlaps(xa, xb, NB) / np.abs(xb - xa)[:, None]
+            for v in range(g.DNV):
+                e = np.array([Cw[0] - Sx, Cw[1] - Sy, zds[v] + zP - Sz])
+                L = g.dx * np.linalg.norm(e) / abs(e[0] if xdrv else e[1])
+                za = (Sz + (bz[v] + zP - Sz) / lam - z_lo) / g.dz
+                zb = (Sz + (bz[v + 1] + zP - Sz) / lam - z_lo) / g.dz
+                lo, hi = np.minimum(za, zb)[..., None], np.maximum(za, zb)[..., None]
+                wz = np.clip(np.minimum(hi, k + 1) - np.maximum(lo, k), 0.0, None) / np.abs(zb - za)[..., None]
+                out[p, u, v] = L * np.einsum("ji,jik,jik->", wx, wz, F)
+    return out
+
+
 CASES = {
     "circular": dict(PN=12, XN=20, YN=18, ZN=10, DNU=30, DNV=12, start=0.13),
     "helical_offset": dict(PN=10, XN=16, YN=22, ZN=14, DNU=28, DNV=10, start=0.4,
@@ -149,3 +205,18 @@ def test_oracle_sat_arithmetic_equals_direct_summation(case):
     want_b = back_direct(g, prj, mask)
     got_b = oracle.dd3_back(g, prj, mask)
     assert np.linalg.norm(got_b - want_b) <= 1e-12 * np.linalg.norm(want_b)
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_branchless_projection_is_close_to_conventional_dd(case):
+    g = G.small(**CASES[case])
+    hx, hy, hz = G.half_extents(g)
+    vol = oracle.ellipsoid_phantom(g, G.shepp_logan_ellipsoids(hx, hy, hz))
+    rng = np.random.default_rng(22)
+    noise = rng.random((g.YN, g.XN, g.ZN)).astype(np.float32)
+    for v in (vol, noise):
+        conv = proj_conventional(g, v)
+        branchless = oracle.dd3_proj(g, v)
+        gap = np.linalg.norm(branchless - conv) / np.linalg.norm(conv)
+        # measured 0.7e-4 .. 1.3e-4 on these scans; the models do differ
+        assert 1e-7 < gap <= 5e-4, gap
