@@ -1,5 +1,5 @@
-"""What the trained warm-start network gains, measured the way the method is judged:
-the data residual ||Ax - b|| / ||b||.  Plain OS-SART runs 20 iterations from zero; the
+"""What the trained warm-start network gains, measured by the data residual the
+solver reports, ||Ax - b|| / ||b||.  Plain OS-SART runs 20 iterations from zero; the
 warm start runs 2 iterations, the network, then OS-SART until its residual reaches the
 plain solve's final one -- in fewer iterations in total, on a held-out phantom."""
 import numpy as np
