@@ -63,6 +63,17 @@ def test_plan_rejects_nonfinite_geometry():
     assert rc == cb.CTLAB_ERR_INVALID_ARG and "non-finite" in msg
 
 
+def test_plan_rejects_oversized_scans_on_host():
+    g = cb.small()
+    g.XN = g.YN = g.ZN = 8000  # 5.1e11 voxels: the size product is checked in FP64
+    rc, msg = _plan_create(g)
+    assert rc == cb.CTLAB_ERR_INVALID_ARG and "too large" in msg
+    g = cb.small()
+    g.zds = np.linspace(-40.0, 40.0, 5000).astype(np.float32)  # 5000 detector rows
+    rc, msg = _plan_create(g)
+    assert rc == cb.CTLAB_ERR_INVALID_ARG and "supported range" in msg
+
+
 def test_plan_rejects_source_inside_volume_extent():
     g = cb.small()
     g.y0 = 2.0  # source inside the 10 mm volume
